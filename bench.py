@@ -1,0 +1,294 @@
+"""Benchmark of the SCF hot path: one Fock (G-matrix) build per step.
+
+Workload (one step): the RHF two-electron Fock build G = 2J[P] - K[P] of
+water with the s/p/d/f even-tempered basis plus the ghost-centre positron
+s/p/d shells (87 shells, 292 Cartesian functions, 7,328,706 unique shell
+quartets before Schwarz screening at 1e-14), from a seeded symmetric
+density.  Every step recomputes every surviving integral (integral-direct)
+and digests it into G.
+
+Metric: shell quartets per second of the Fock build (whole job), and
+seconds per SCF-iteration Fock build.  With --gpus N (torchrun) each rank
+owns every N-th quartet of each class, builds its partial accumulator and
+the partials are summed with one NCCL all-reduce before the symmetrising
+finish (the reference's MPI_Reduce of G, rhfscf_mpi.c:36).
+
+--impl reference times the reference's own CPU Fock build (oracle/_ref,
+serial C, one core) on the same workload: the reference writes the ERIs to
+disk once (untimed set-up) and each step digests one 1-GiB ERI file with
+rhf_form_gmatrix (scfaux.c:429-552); its throughput is scaled to quartets
+by the share of all integral records that file holds.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 functions), RHF Fock build"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="patgpu", choices=["patgpu", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tau", type=float, default=1e-14)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        out.update(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                   reasons=sorted(reasons), samples=len(rows))
+        return out
+
+
+# ------------------------------------------------------------- reference
+def reference_fock(steps: int, warmup: int):
+    """The reference's own Fock build on the host (see module docstring)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import patref   # CPU-baseline leg: the reference binary and its runner
+    from patmol_b200 import configs, workload
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return None, "oracle/_ref/ref_harness was not built"
+    b = configs.water_spdf_positron()
+    qtotal = sum(workload.quartet_class_counts(b).values())
+    with tempfile.TemporaryDirectory(prefix="patref_bench_") as d:
+        b.write_patin(os.path.join(d, "patin.dat"))
+        r = subprocess.run([harness, "bench1", str(steps), str(warmup)], cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            return None, "reference harness failed: " + r.stderr[-300:].replace("\n", " ")
+        res = json.loads(r.stdout.strip().splitlines()[-1])
+    frac = res["file_records"] / res["records"]
+    t = res["gmat_seconds_per_call"]
+    qps = qtotal * frac / t
+    return {"value": qps, "unit": "quartets/s", "cores": 1, "kind": "reference",
+            "sample": (f"reference rhf_form_gmatrix over one 1-GiB ERI file ({res['file_records']} of "
+                       f"{res['records']} records, scaled to {qtotal} quartets); {t:.3f} s per file; "
+                       f"ERI generation {res['eri_seconds']:.1f} s untimed"),
+            "s_per_fock_build": t / frac, "eri_seconds": res["eri_seconds"]}, None
+
+
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    res, err = reference_fock(a.steps, a.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    line = {"metric": "ERI quartets/s (Fock build)", "value": res["value"], "unit": "quartets/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": res["s_per_fock_build"] * 1e3, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "density": "seeded"},
+            "impl": "reference", "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------- GPU
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from patmol_b200 import configs, gpu, workload
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+
+    b = configs.water_spdf_positron()
+    n = b.norb
+    no2 = n * (n + 1) // 2
+    G = gpu.GpuBasis(b, schwarz_tau=a.tau)
+    G.two_electron_ints(0, rank, world)
+    st = G.stats()
+    counts = G.class_counts()
+    my_flops = workload.fock_flops(counts, "rhf")
+    my_q = st["quartets"]
+    tot = torch.tensor([my_q, my_flops], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot)
+    total_q, total_flops = int(tot[0].item()), float(tot[1].item())
+
+    rng = np.random.default_rng(1234)
+    P_host = torch.from_numpy(rng.normal(scale=0.05, size=no2)).pin_memory()
+    G_host = torch.empty(no2, dtype=torch.float64).pin_memory()
+    P = P_host.to(dev)
+    A = torch.empty(n * n, dtype=torch.float64, device=dev)
+    Gd = torch.empty(no2, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    def step():
+        G.rhf_accumulate_device(P.data_ptr(), A.data_ptr(), sh)
+        if world > 1:
+            dist.all_reduce(A)
+        G.finish_gmatrix_device(A.data_ptr(), Gd.data_ptr(), sh)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    kern_ns = 0.0
+    launches = 0
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    for i in range(a.steps):
+        flush.fill_(float(i))                      # evict L2 between steps (not timed)
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        kns, nl = G.last_timing()
+        kern_ns += kns
+        launches += nl + 2                        # class kernels + unpack + finish
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / a.steps
+    kern_ms = kern_ns / 1e6 / a.steps
+
+    # end to end through the public C ABI: pinned host P in, host G out
+    e2e_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2e_ev[0].record(stream)
+    for i in range(a.steps):
+        P.copy_(P_host, non_blocking=True)
+        step()
+        G_host.copy_(Gd, non_blocking=True)
+    e2e_ev[1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2e_ev[0].elapsed_time(e2e_ev[1]) / a.steps
+    clk = clocks.stop()
+
+    t = torch.tensor([step_ms, e2e_ms, kern_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, e2e_ms, kern_ms = (float(x) for x in t.tolist())
+
+    line = None
+    if rank == 0:
+        peak = gpu.fp64_peak_tflops()
+        achieved = my_flops / (kern_ms * 1e-3) / 1e12 if kern_ms > 0 else None
+        line = {
+            "metric": "ERI quartets/s (Fock build)",
+            "value": total_q / (step_ms * 1e-3),
+            "unit": "quartets/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": step_ms,
+            "s_per_scf_iteration_fock": step_ms * 1e-3,
+            "higher_is_better": True,
+            "scaling": "strong",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "quartets": total_q, "quartets_unscreened": st["unscreened"],
+                       "schwarz_tau": a.tau, "basis_functions": n, "density": "seeded N(0,0.05^2)",
+                       "l2": "flushed between steps (256 MB write, untimed)",
+                       "parallelism": f"quartet split x{world}" + (" + NCCL all-reduce" if world > 1 else "")},
+            "e2e": {"value": total_q / (e2e_ms * 1e-3), "unit": "quartets/s",
+                    "h2d_bytes_per_step": no2 * 8, "d2h_bytes_per_step": no2 * 8,
+                    "path": "pinned P -> patgpu_rhf_accumulate_device -> patgpu_finish_gmatrix_device -> pinned G"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": "measured FP64 FMA probe (patgpu_fp64_peak), this GPU, this run",
+                         "algorithmic_flops_per_step": my_flops,
+                         "kernel_ms_per_step": kern_ms},
+            "gpu_launches": launches,
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        if world == 1 and not a.no_cpu_baseline:
+            res, err = reference_fock(2, 1)
+            line["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                                    if res else {"unavailable": err})
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

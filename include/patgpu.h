@@ -1,0 +1,167 @@
+/*
+ * patgpu.h -- C ABI of libpatgpu.so, the B200 (sm_100a) implementation of
+ * Patmol's SCF hot path: two-electron integrals over shell quartets (Rys
+ * quadrature) fused with their digestion into the G matrix, and the
+ * distributed-positron-model / one-electron integrals.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the reference's exact signatures.  A
+ *     program built from the reference's host sources links these instead
+ *     of twoints.c, dpmints.c and the two G builds of scfaux.c.  They read
+ *     the basis through the reference's accessors (shells(), centers(),
+ *     number_of_shells(), ... basis.h:16-50), which the host program
+ *     provides.  Matrices are packed lower triangles, row-major
+ *     (ij = i(i+1)/2 + j, scfaux.c:452-456); P is the RHF half density.
+ *
+ *  2. Explicit entry points (patgpu_*) taking plain arrays, used by the
+ *     drop-in layer, the Python host mirror and the tests.  Every one
+ *     returns 0 on success or a negative PATGPU_E* code; the message of the
+ *     last failure on the calling thread is patgpu_error_message().
+ *
+ * No entry point has a CPU fallback: without a usable CUDA device they fail
+ * with PATGPU_ENODEV.
+ */
+#ifndef PATGPU_H
+#define PATGPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- drop-in */
+/* The reference's ERI file handle (erifs.h:14-18).  The GPU library keeps
+ * integral-direct state keyed by the handle's address and writes no files:
+ * after two_electron_ints, tfiles->nfiles is 0. */
+#ifndef _ERIFS_H_
+typedef struct {
+    int rank, nproc, nfiles;
+    int *numints;
+    char *basename;
+} ERIFS;
+#endif
+
+/* Replaces two_electron_ints (twoints.h:14, twoints.c:188-418): snapshots the
+ * current basis (shells with nst == 0 contribute nothing), builds shell
+ * pairs, Schwarz bounds and the screened quartet list of every shell
+ * quartet whose largest shell index is >= start, and binds them to tfiles. */
+void two_electron_ints(ERIFS *tfiles, int start);
+
+/* Replaces rhf_form_gmatrix (scfaux.h:22-23, scfaux.c:429-552):
+ * Gmat += 2 J[P] - K[P] over the quartets bound to tfiles. */
+void rhf_form_gmatrix(const ERIFS *tfiles, const double *Pmat, double *Gmat);
+
+/* Replaces uhf_form_gmatrix (scfaux.h:24-26, scfaux.c:555-714):
+ * GmatA += J[PA+PB] - K[PA], GmatB += J[PA+PB] - K[PB]. */
+void uhf_form_gmatrix(const ERIFS *tfiles, const double *PmatA, const double *PmatB,
+                      double *GmatA, double *GmatB);
+
+/* Replaces dpm_ints (dpmints.h:12, dpmints.c:121-199): hmat -= V_DPM, the
+ * six-Gaussian model potential centred on centre skip_center(). */
+void dpm_ints(double *hmat);
+
+/* Replaces one_electron_ints (oneints.h:10, oneints.c:139-234):
+ * S, T and H = T + V (all centres but skip_center()). */
+void one_electron_ints(double *Smat, double *Tmat, double *Hmat);
+
+/* ------------------------------------------------------------- explicit */
+typedef struct patgpu_basis *patgpu_handle;
+
+enum {
+    PATGPU_OK = 0,
+    PATGPU_EINVAL = -1,      /* bad argument */
+    PATGPU_ENODEV = -2,      /* no CUDA device */
+    PATGPU_ECUDA = -3,       /* a CUDA call failed */
+    PATGPU_EUNSUPPORTED = -4,/* angular momentum above f */
+    PATGPU_ENOMEM = -5,
+    PATGPU_ESTATE = -6,      /* call order (e.g. no quartets built) */
+};
+
+int patgpu_last_error(void);
+const char *patgpu_error_message(void);
+
+/* Basis snapshot.  Per shell: l, centre, first basis function, Cartesian
+ * component count (0 = contributes nothing, as the reference's DPM shells),
+ * primitive range [prim_off[s], prim_off[s+1]) into alpha/coef; coef holds
+ * the normalised contraction coefficients (what shells() returns after
+ * normalize_shell, shell.c:26-56).  Per centre charge and xyz (bohr).
+ * skipcen is left out of V and carries the DPM potential.  schwarz_tau:
+ * quartets with Q_ab Q_cd < tau are skipped (0 disables screening).
+ * Builds pairs and Schwarz bounds on the current CUDA device. */
+int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off, const int *nst,
+                        const int *prim_off, const double *alpha, const double *coef, int ncen,
+                        const double *charge, const double *xyz, int skipcen, double schwarz_tau,
+                        patgpu_handle *out);
+int patgpu_basis_destroy(patgpu_handle h);
+
+/* Which quartets this handle owns: those whose largest shell index is
+ * >= start_shell (the reference's `start`, twoints.c:228), and of those
+ * every nranks-th of each class starting at rank (static split across
+ * GPUs).  Rebuilds the quartet list. */
+int patgpu_set_quartets(patgpu_handle h, int start_shell, int rank, int nranks);
+
+/* Host-buffer Fock builds (packed lower triangles; outputs accumulate). */
+int patgpu_rhf_gmatrix(patgpu_handle h, const double *P, double *G);
+int patgpu_uhf_gmatrix(patgpu_handle h, const double *PA, const double *PB, double *GA, double *GB);
+/* J[P] and K[P] separately (packed; accumulate). */
+int patgpu_jk(patgpu_handle h, const double *P, double *J, double *K);
+
+/* Device-resident Fock build: dP and dG are device pointers to packed
+ * triangles; dG is overwritten (not accumulated).  stream is the
+ * cudaStream_t to enqueue on, used as given (NULL = the legacy default
+ * stream).  Enqueues only; the caller synchronises. */
+int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, void *stream);
+/* Same, leaving the unsymmetrised n x n accumulator in dA (G = A + A^T),
+ * for callers that reduce partial results across GPUs before finishing. */
+int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, void *stream);
+int patgpu_finish_gmatrix_device(patgpu_handle h, const double *dA, double *dG, void *stream);
+
+/* Integrals of arbitrary shell quartets (a b | c d), nq x 4 shell indices;
+ * out receives, per quartet in order, na*nb*nc*nd values indexed
+ * ((ia nb + ib) nc + ic) nd + id with the reference's component order and
+ * factors.  Host buffers. */
+int patgpu_eri_quartets(patgpu_handle h, int nq, const int *shells4, double *out);
+
+/* One-electron S, T, H = T + V (packed, overwritten) and H -= V_DPM. */
+int patgpu_oneints(patgpu_handle h, double *S, double *T, double *H);
+int patgpu_dpm(patgpu_handle h, double *H);
+/* The same without a handle (no pair or quartet set-up): any of S/T/H may
+ * be NULL together (then only Hdpm is formed), Hdpm may be NULL. */
+int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, const int *nst,
+                   const int *prim_off, const double *alpha, const double *coef, int ncen,
+                   const double *charge, const double *xyz, int skipcen, double *S, double *T,
+                   double *H, double *Hdpm);
+
+/* Sizes of the handle: [0] basis functions, [1] shell pairs, [2] quartets
+ * owned, [3] classes with work, [4] quartets before screening. */
+int patgpu_stats(patgpu_handle h, long long *out5);
+/* Per class with work: l of the four shells and the quartet count. */
+int patgpu_class_counts(patgpu_handle h, int max, int *l4, long long *counts);
+/* Nanoseconds of the last Fock build's class kernels (CUDA events on the
+ * handle's stream, first kernel start to last kernel end), and the number
+ * of kernels it launched. */
+int patgpu_last_timing(patgpu_handle h, double *kernel_ns, int *launches);
+
+/* Measured dense FP64 FMA throughput of the current device (TFLOP/s), the
+ * denominator of the kernels' roofline fraction. */
+int patgpu_fp64_peak(double *tflops);
+
+/* Host evaluation of the Rys root tables the kernels use (no device
+ * needed): x = t^2 nodes and weights of the n-point rule at T. */
+int patgpu_rys_host(int n, double T, double *x, double *w);
+
+/* Make device (index modulo the device count) current for this thread. The
+ * drop-in layer calls it once with PATGPU_DEVICE or the launcher's
+ * node-local rank (OMPI_COMM_WORLD_LOCAL_RANK, MPI_LOCALRANKID,
+ * SLURM_LOCALID, LOCAL_RANK) when one is set. */
+int patgpu_select_device(int index);
+
+/* Drop every handle the drop-in layer created. */
+void patgpu_release_all(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

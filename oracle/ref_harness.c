@@ -23,6 +23,9 @@
  *                               when a ghost centre sits on the positron).
  *   ref_harness bench K         times two_electron_ints once and K calls of
  *                               rhf_form_gmatrix, prints one JSON line.
+ *   ref_harness bench1 K W      the same, but each call digests only the
+ *                               first ERI file (a bounded sample of the
+ *                               Fock build), after W untimed calls.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -374,6 +377,30 @@ int main(int argc, char **argv)
         tg = (now_s() - t0) / (K > 0 ? K : 1);
         printf("{\"eri_seconds\": %.6f, \"gmat_seconds_per_call\": %.6f, \"records\": %zu, \"norb\": %d, \"nshell\": %d}\n",
                secs, tg, nrec, n, number_of_shells());
+        clean_ERIFS(e);
+        return 0;
+    }
+    if (!strcmp(argv[1], "bench1") && argc >= 4) {
+        int k, K = atoi(argv[2]), W = atoi(argv[3]);
+        double *P = dalloc(no2), *G = dalloc(no2), secs, t0, tg;
+        ERIFS *e = make_eris(0, "MINTS.DAT", &secs), view;
+        size_t nrec = 0;
+        for (k = 0; k < e->nfiles; ++k) nrec += e->numints[k];
+        view = *e;
+        view.nfiles = e->nfiles > 0 ? 1 : 0;      /* file 0 only */
+        for (k = 0; k < no2; ++k) P[k] = 1.0 / (1.0 + k % 7);
+        for (k = 0; k < W; ++k) {
+            memset(G, 0, sizeof(double) * no2);
+            rhf_form_gmatrix(&view, P, G);
+        }
+        t0 = now_s();
+        for (k = 0; k < K; ++k) {
+            memset(G, 0, sizeof(double) * no2);
+            rhf_form_gmatrix(&view, P, G);
+        }
+        tg = (now_s() - t0) / (K > 0 ? K : 1);
+        printf("{\"eri_seconds\": %.6f, \"gmat_seconds_per_call\": %.6f, \"records\": %zu, \"file_records\": %d, \"nfiles\": %d, \"norb\": %d}\n",
+               secs, tg, nrec, e->nfiles ? e->numints[0] : 0, e->nfiles, n);
         clean_ERIFS(e);
         return 0;
     }

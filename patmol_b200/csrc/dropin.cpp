@@ -1,0 +1,189 @@
+// dropin.cpp -- the reference's integral and Fock-build entry points
+// (twoints.h:14, scfaux.h:22-26, dpmints.h:12, oneints.h:10) on the GPU.
+//
+// They read the basis through the reference's accessors (basis.h:16-50),
+// which the host program defines; the declarations below are weak so that
+// the library also loads in programs that have no reference basis module
+// (the explicit patgpu_* layer needs none), in which case these entry
+// points report the missing accessors through fatalError.
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "../../include/patgpu.h"
+
+// Layouts of the reference's basis records (shell.h:9-13, center.h:5-7).
+typedef struct {
+    int npr, lsh, cen, off, nst;
+    double *al;
+    double *co;
+} Shell;
+typedef struct {
+    double q, r[3];
+} Center;
+
+extern "C" {
+const Shell *shells() __attribute__((weak));
+const Center *centers() __attribute__((weak));
+int number_of_shells() __attribute__((weak));
+int number_of_centers() __attribute__((weak));
+int skip_center() __attribute__((weak));
+void fatalError(const char *message) __attribute__((weak));
+}
+
+namespace {
+
+std::mutex g_lock;
+std::map<const ERIFS *, patgpu_handle> g_handles;
+
+[[noreturn]] void die(const char *what)
+{
+    char buf[768];
+    snprintf(buf, sizeof buf, "patgpu: %s: %s", what, patgpu_error_message());
+    if (fatalError) fatalError(buf);   // util.c:21-26 prints and exits
+    fprintf(stderr, "FATAL ERROR: %s\n", buf);
+    exit(EXIT_FAILURE);
+}
+
+void need_accessors()
+{
+    if (!shells || !centers || !number_of_shells || !number_of_centers || !skip_center) {
+        fprintf(stderr, "FATAL ERROR: patgpu drop-in entry called without the reference's basis module\n");
+        exit(EXIT_FAILURE);
+    }
+}
+
+// Snapshot of the basis the reference holds right now.
+struct Snap {
+    std::vector<int> l, cen, off, nst, poff;
+    std::vector<double> al, co, q, xyz;
+    int nsh = 0, ncen = 0, skip = 0;
+};
+
+Snap snapshot()
+{
+    need_accessors();
+    Snap s;
+    const Shell *sh = shells();
+    const Center *c = centers();
+    s.nsh = number_of_shells();
+    s.ncen = number_of_centers();
+    s.skip = skip_center();
+    s.poff.push_back(0);
+    for (int i = 0; i < s.nsh; ++i) {
+        s.l.push_back(sh[i].lsh);
+        s.cen.push_back(sh[i].cen);
+        s.off.push_back(sh[i].off);
+        s.nst.push_back(sh[i].nst);
+        for (int k = 0; k < sh[i].npr; ++k) {
+            s.al.push_back(sh[i].al[k]);
+            s.co.push_back(sh[i].co[k]);
+        }
+        s.poff.push_back((int)s.al.size());
+    }
+    for (int i = 0; i < s.ncen; ++i) {
+        s.q.push_back(c[i].q);
+        s.xyz.insert(s.xyz.end(), c[i].r, c[i].r + 3);
+    }
+    return s;
+}
+
+// One GPU per MPI rank: the reference's MPI program (patmpi) runs one process
+// per rank; pick the device from the launcher's node-local rank.
+void select_device_once()
+{
+    static bool done = false;
+    if (done) return;
+    done = true;
+    const char *vars[] = {"PATGPU_DEVICE", "OMPI_COMM_WORLD_LOCAL_RANK", "MPI_LOCALRANKID", "SLURM_LOCALID",
+                          "LOCAL_RANK"};
+    for (const char *v : vars) {
+        const char *e = getenv(v);
+        if (e && *e) {
+            patgpu_select_device(atoi(e));
+            return;
+        }
+    }
+}
+
+patgpu_handle make_handle(const Snap &s, double tau)
+{
+    select_device_once();
+    patgpu_handle h = nullptr;
+    if (patgpu_basis_create(s.nsh, s.l.data(), s.cen.data(), s.off.data(), s.nst.data(), s.poff.data(),
+                            s.al.data(), s.co.data(), s.ncen, s.q.data(), s.xyz.data(), s.skip, tau, &h))
+        die("building the basis on the GPU");
+    return h;
+}
+
+double schwarz_tau()
+{
+    const char *e = getenv("PATGPU_SCHWARZ");
+    return e ? atof(e) : 1e-14;
+}
+
+}  // namespace
+
+extern "C" {
+
+void two_electron_ints(ERIFS *tfiles, int start)
+{
+    if (!tfiles) die("two_electron_ints: null handle");
+    std::lock_guard<std::mutex> g(g_lock);
+    auto it = g_handles.find(tfiles);
+    if (it != g_handles.end()) {
+        patgpu_basis_destroy(it->second);
+        g_handles.erase(it);
+    }
+    Snap s = snapshot();
+    patgpu_handle h = make_handle(s, schwarz_tau());
+    int rank = tfiles->rank, nproc = tfiles->nproc > 0 ? tfiles->nproc : 1;
+    if (patgpu_set_quartets(h, start, rank % nproc, nproc)) die("two_electron_ints");
+    g_handles[tfiles] = h;
+    tfiles->nfiles = 0;   // integral-direct: no ERI files
+}
+
+void rhf_form_gmatrix(const ERIFS *tfiles, const double *Pmat, double *Gmat)
+{
+    std::lock_guard<std::mutex> g(g_lock);
+    auto it = g_handles.find(tfiles);
+    if (it == g_handles.end()) die("rhf_form_gmatrix before two_electron_ints");
+    if (patgpu_rhf_gmatrix(it->second, Pmat, Gmat)) die("rhf_form_gmatrix");
+}
+
+void uhf_form_gmatrix(const ERIFS *tfiles, const double *PmatA, const double *PmatB, double *GmatA, double *GmatB)
+{
+    std::lock_guard<std::mutex> g(g_lock);
+    auto it = g_handles.find(tfiles);
+    if (it == g_handles.end()) die("uhf_form_gmatrix before two_electron_ints");
+    if (patgpu_uhf_gmatrix(it->second, PmatA, PmatB, GmatA, GmatB)) die("uhf_form_gmatrix");
+}
+
+void dpm_ints(double *hmat)
+{
+    select_device_once();
+    Snap s = snapshot();
+    if (patgpu_onebody(s.nsh, s.l.data(), s.cen.data(), s.off.data(), s.nst.data(), s.poff.data(), s.al.data(),
+                       s.co.data(), s.ncen, s.q.data(), s.xyz.data(), s.skip, nullptr, nullptr, nullptr, hmat))
+        die("dpm_ints");
+}
+
+void one_electron_ints(double *Smat, double *Tmat, double *Hmat)
+{
+    select_device_once();
+    Snap s = snapshot();
+    if (patgpu_onebody(s.nsh, s.l.data(), s.cen.data(), s.off.data(), s.nst.data(), s.poff.data(), s.al.data(),
+                       s.co.data(), s.ncen, s.q.data(), s.xyz.data(), s.skip, Smat, Tmat, Hmat, nullptr))
+        die("one_electron_ints");
+}
+
+void patgpu_release_all(void)
+{
+    std::lock_guard<std::mutex> g(g_lock);
+    for (auto &kv : g_handles) patgpu_basis_destroy(kv.second);
+    g_handles.clear();
+}
+
+}  // extern "C"

@@ -1,0 +1,820 @@
+// library.cu -- host orchestration and the explicit C ABI of libpatgpu.so:
+// basis snapshot, shell pairs, Schwarz bounds, class-sorted screened quartet
+// lists, and the Fock builds that launch the class kernels of eri.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/patgpu.h"
+#include "eri.cuh"
+#include "onebody.cuh"
+#include "rys_table.h"
+
+namespace pg {
+
+// ------------------------------------------------------------------ errors
+static thread_local int t_err = 0;
+static thread_local char t_msg[512] = "";
+
+int fail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_msg, sizeof(t_msg), fmt, ap);
+    va_end(ap);
+    t_err = code;
+    return code;
+}
+
+#define PG_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(PATGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------ device memory
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t b)
+    {
+        if (b <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, b ? b : 16);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+template <class T>
+static cudaError_t upload(DBuf &b, const std::vector<T> &v, cudaStream_t s)
+{
+    cudaError_t e = b.ensure(sizeof(T) * v.size());
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s);
+}
+
+// ------------------------------------------------------------------ tables
+static std::once_flag g_rys_once;
+static DBuf *g_rys_coef = nullptr;   // per process (one device per process)
+static int g_rys_status = 0;
+
+static RysConst host_rys_const()
+{
+    RysConst rc{};
+    for (int n = 0; n <= RYS_NMAX; ++n) {
+        rc.tmax[n] = rys_tmax[n];
+        rc.off[n] = rys_off[n];
+        for (int i = 0; i < RYS_NMAX; ++i) {
+            rc.lag_x[n][i] = rys_lag_x[n][i];
+            rc.lag_w[n][i] = rys_lag_w[n][i];
+        }
+    }
+    return rc;
+}
+
+static int init_tables()
+{
+    std::call_once(g_rys_once, [] {
+        g_rys_coef = new DBuf();
+        if (g_rys_coef->ensure(sizeof(double) * rys_ncoef) != cudaSuccess ||
+            cudaMemcpy(g_rys_coef->p, rys_coef_host, sizeof(double) * rys_ncoef, cudaMemcpyHostToDevice) !=
+                cudaSuccess ||
+            upload_rys_constants(host_rys_const()) != cudaSuccess || upload_onebody_constants() != cudaSuccess)
+            g_rys_status = -1;
+    });
+    if (g_rys_status) return fail(PATGPU_ECUDA, "uploading the Rys tables failed");
+    return 0;
+}
+
+// ------------------------------------------------------------------ handle
+struct ClassWork {
+    int la, lb, lc, ld;
+    long long offset, count;
+};
+
+static int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+}  // namespace pg
+
+struct patgpu_basis {
+    // snapshot
+    int nsh = 0, ncen = 0, n = 0, skipcen = 0;
+    std::vector<int> l, cen, off, nst, poff;
+    std::vector<double> al, co, q, xyz;
+    double tau = 0.0;
+    int start_shell = 0, rank = 0, nranks = 1;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    // pairs (class-sorted)
+    int npair = 0;
+    std::vector<int> psa, psb, pfa, pfb, pcls, pstart, pnum;
+    std::vector<double> pax, pay, paz, pabx, paby, pabz, Q;
+    std::vector<double> pp_p, pp_px, pp_py, pp_pz, pp_K, pp_cut;
+    std::vector<int> class_begin;   // pairs of class c: [class_begin[c], class_begin[c+1])
+    pg::DBuf d_psa, d_psb, d_pfa, d_pfb, d_pax, d_pay, d_paz, d_pabx, d_paby, d_pabz, d_pstart, d_pnum;
+    pg::DBuf d_pp_p, d_pp_px, d_pp_py, d_pp_pz, d_pp_K, d_pp_cut;
+    // quartets
+    std::vector<pg::ClassWork> work;
+    pg::DBuf d_quart;
+    long long nquart = 0, nquart_unscreened = 0;
+    // work buffers
+    pg::DBuf d_D0, d_D1, d_A0, d_A1, d_Pk0, d_Pk1, d_Gk0, d_Gk1, d_err;
+    std::vector<double> h_stage;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ns = 0.0;
+    int last_launches = 0;
+
+    pg::EriArgs base_args() const
+    {
+        pg::EriArgs a{};
+        a.pr.sa = d_psa.as<int>();
+        a.pr.sb = d_psb.as<int>();
+        a.pr.fa = d_pfa.as<int>();
+        a.pr.fb = d_pfb.as<int>();
+        a.pr.ax = d_pax.as<double>();
+        a.pr.ay = d_pay.as<double>();
+        a.pr.az = d_paz.as<double>();
+        a.pr.abx = d_pabx.as<double>();
+        a.pr.aby = d_paby.as<double>();
+        a.pr.abz = d_pabz.as<double>();
+        a.pr.pstart = d_pstart.as<int>();
+        a.pr.pnum = d_pnum.as<int>();
+        a.pp.p = d_pp_p.as<double>();
+        a.pp.px = d_pp_px.as<double>();
+        a.pp.py = d_pp_py.as<double>();
+        a.pp.pz = d_pp_pz.as<double>();
+        a.pp.K = d_pp_K.as<double>();
+        a.pp.cut = d_pp_cut.as<double>();
+        a.n = n;
+        a.rys_coef = pg::g_rys_coef->as<double>();
+        a.prim_cut = 1e-15;
+        a.err = d_err.as<int>();
+        return a;
+    }
+};
+
+namespace pg {
+
+static int build_pairs(patgpu_basis *h)
+{
+    struct Tmp {
+        int a, b, cls;
+    };
+    std::vector<Tmp> t;
+    for (int i = 0; i < h->nsh; ++i) {
+        if (!h->nst[i]) continue;
+        for (int j = 0; j <= i; ++j) {
+            if (!h->nst[j]) continue;
+            int a = i, b = j;
+            if (h->l[i] < h->l[j]) std::swap(a, b);   // larger l first (twoints.c:249-266)
+            t.push_back({a, b, pair_class(h->l[a], h->l[b])});
+        }
+    }
+    std::stable_sort(t.begin(), t.end(), [](const Tmp &x, const Tmp &y) { return x.cls < y.cls; });
+    h->npair = (int)t.size();
+    h->psa.clear(); h->psb.clear(); h->pfa.clear(); h->pfb.clear(); h->pcls.clear();
+    h->pstart.clear(); h->pnum.clear(); h->pax.clear(); h->pay.clear(); h->paz.clear();
+    h->pabx.clear(); h->paby.clear(); h->pabz.clear();
+    h->pp_p.clear(); h->pp_px.clear(); h->pp_py.clear(); h->pp_pz.clear(); h->pp_K.clear(); h->pp_cut.clear();
+    h->class_begin.assign(11, 0);
+    for (auto &x : t) h->class_begin[x.cls + 1]++;
+    for (int c = 0; c < 10; ++c) h->class_begin[c + 1] += h->class_begin[c];
+    for (auto &x : t) {
+        const double *A = &h->xyz[3 * h->cen[x.a]], *B = &h->xyz[3 * h->cen[x.b]];
+        double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+        double ab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+        h->psa.push_back(x.a);
+        h->psb.push_back(x.b);
+        h->pfa.push_back(h->off[x.a]);
+        h->pfb.push_back(h->off[x.b]);
+        h->pcls.push_back(x.cls);
+        h->pax.push_back(A[0]); h->pay.push_back(A[1]); h->paz.push_back(A[2]);
+        h->pabx.push_back(AB[0]); h->paby.push_back(AB[1]); h->pabz.push_back(AB[2]);
+        h->pstart.push_back((int)h->pp_p.size());
+        int np = 0;
+        for (int i = h->poff[x.a]; i < h->poff[x.a + 1]; ++i)
+            for (int j = h->poff[x.b]; j < h->poff[x.b + 1]; ++j) {
+                double ea = h->al[i], eb = h->al[j], p = ea + eb;
+                double s = std::exp(-ea * eb * ab2 / p);
+                h->pp_p.push_back(p);
+                h->pp_px.push_back((ea * A[0] + eb * B[0]) / p);
+                h->pp_py.push_back((ea * A[1] + eb * B[1]) / p);
+                h->pp_pz.push_back((ea * A[2] + eb * B[2]) / p);
+                h->pp_cut.push_back(s / p);
+                h->pp_K.push_back(h->co[i] * h->co[j] * s / p);
+                ++np;
+            }
+        h->pnum.push_back(np);
+    }
+    cudaStream_t s = h->stream;
+    cudaError_t e = cudaSuccess;
+#define UP(buf, vec) if (e == cudaSuccess) e = upload(h->buf, h->vec, s)
+    UP(d_psa, psa); UP(d_psb, psb); UP(d_pfa, pfa); UP(d_pfb, pfb);
+    UP(d_pax, pax); UP(d_pay, pay); UP(d_paz, paz); UP(d_pabx, pabx); UP(d_paby, paby); UP(d_pabz, pabz);
+    UP(d_pstart, pstart); UP(d_pnum, pnum);
+    UP(d_pp_p, pp_p); UP(d_pp_px, pp_px); UP(d_pp_py, pp_py); UP(d_pp_pz, pp_pz); UP(d_pp_K, pp_K);
+    UP(d_pp_cut, pp_cut);
+#undef UP
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(PATGPU_ECUDA, "pair upload: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+static void class_ls(int cls, int &la, int &lb)
+{
+    la = 0;
+    while ((la + 1) * (la + 2) / 2 <= cls) ++la;
+    lb = cls - la * (la + 1) / 2;
+}
+
+// Run export-mode kernels over explicit (u, v) pair quartets; out receives
+// the blocks in kernel orientation at the offsets returned in offs.
+static int export_pairs(patgpu_basis *h, const std::vector<int2> &quart, std::vector<double> &out,
+                        std::vector<long long> &offs, double prim_cut = 1e-15)
+{
+    // group by class pair, keep the caller's order inside each group
+    const size_t nq = quart.size();
+    offs.assign(nq, 0);
+    long long total = 0;
+    std::vector<size_t> order(nq);
+    for (size_t i = 0; i < nq; ++i) order[i] = i;
+    auto key = [&](size_t i) { return h->pcls[quart[i].x] * 16 + h->pcls[quart[i].y]; };
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return key(x) < key(y); });
+    std::vector<int2> sorted(nq);
+    std::vector<long long> soff(nq);
+    for (size_t k = 0; k < nq; ++k) {
+        size_t i = order[k];
+        sorted[k] = quart[i];
+        int la, lb, lc, ld;
+        class_ls(h->pcls[quart[i].x], la, lb);
+        class_ls(h->pcls[quart[i].y], lc, ld);
+        soff[k] = total;
+        offs[i] = total;
+        total += (long long)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+    }
+    DBuf dq, dout, doff;
+    cudaStream_t s = h->stream;
+    PG_CUDA(upload(dq, sorted, s));
+    PG_CUDA(upload(doff, soff, s));
+    PG_CUDA(dout.ensure(sizeof(double) * (size_t)std::max<long long>(total, 1)));
+    size_t k = 0;
+    while (k < nq) {
+        size_t e = k;
+        while (e < nq && key(order[e]) == key(order[k])) ++e;
+        int la, lb, lc, ld;
+        class_ls(h->pcls[sorted[k].x], la, lb);
+        class_ls(h->pcls[sorted[k].y], lc, ld);
+        EriArgs a = h->base_args();
+        a.mode = MODE_EXPORT;
+        a.prim_cut = prim_cut;
+        a.quart = dq.as<int2>() + k;
+        a.nquart = (long long)(e - k);
+        a.out = dout.as<double>();
+        a.out_off = doff.as<long long>() + k;
+        PG_CUDA(launch_eri_class(la, lb, lc, ld, a, s, h->num_sms));
+        k = e;
+    }
+    out.resize((size_t)total);
+    if (total) PG_CUDA(cudaMemcpyAsync(out.data(), dout.p, sizeof(double) * total, cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+static int build_schwarz(patgpu_basis *h)
+{
+    std::vector<int2> diag(h->npair);
+    for (int u = 0; u < h->npair; ++u) diag[u] = make_int2(u, u);
+    std::vector<double> out;
+    std::vector<long long> offs;
+    // no primitive cut here: a pair whose own diagonal falls below the cut
+    // can still meet a diffuse pair above it, so its bound must be exact
+    int rc = export_pairs(h, diag, out, offs, 0.0);
+    if (rc) return rc;
+    h->Q.assign(h->npair, 0.0);
+    for (int u = 0; u < h->npair; ++u) {
+        int la, lb;
+        class_ls(h->pcls[u], la, lb);
+        const int na = ncart(la), nb = ncart(lb);
+        double m = 0.0;
+        for (int i = 0; i < na; ++i)
+            for (int j = 0; j < nb; ++j) {
+                double v = out[offs[u] + (((size_t)i * nb + j) * na + i) * nb + j];
+                m = std::max(m, std::fabs(v));
+            }
+        h->Q[u] = std::sqrt(m);
+    }
+    return 0;
+}
+
+static int build_quartets(patgpu_basis *h)
+{
+    h->work.clear();
+    std::vector<int2> all;
+    long long unscreened = 0;
+    for (int cu = 0; cu < 10; ++cu)
+        for (int cv = 0; cv <= cu; ++cv) {
+            const int u0 = h->class_begin[cu], u1 = h->class_begin[cu + 1];
+            const int v0 = h->class_begin[cv], v1 = h->class_begin[cv + 1];
+            if (u0 == u1 || v0 == v1) continue;
+            ClassWork w;
+            class_ls(cu, w.la, w.lb);
+            class_ls(cv, w.lc, w.ld);
+            w.offset = (long long)all.size();
+            long long k = 0;
+            for (int u = u0; u < u1; ++u) {
+                const int vend = (cu == cv) ? u + 1 : v1;
+                const int mu = std::max(h->psa[u], h->psb[u]);
+                for (int v = v0; v < vend; ++v) {
+                    ++unscreened;
+                    if (h->tau > 0.0 && h->Q[u] * h->Q[v] < h->tau) continue;
+                    if (std::max(mu, std::max(h->psa[v], h->psb[v])) < h->start_shell) continue;
+                    if ((k++ % h->nranks) != h->rank) continue;
+                    all.push_back(make_int2(u, v));
+                }
+            }
+            w.count = (long long)all.size() - w.offset;
+            if (w.count) h->work.push_back(w);
+        }
+    h->nquart = (long long)all.size();
+    h->nquart_unscreened = unscreened;
+    PG_CUDA(upload(h->d_quart, all, h->stream));
+    PG_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+// ------------------------------------------------------- small kernels
+__global__ void unpack_kernel(const double *__restrict__ pk, double *__restrict__ full, int n)
+{
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)n * n;
+    for (; idx < tot; idx += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(idx / n), j = (int)(idx % n);
+        int r = i > j ? i : j, c = i > j ? j : i;
+        full[idx] = pk[(long long)r * (r + 1) / 2 + c];
+    }
+}
+
+// packed[ij] = A[i][j] + A[j][i] (j <= i)
+__global__ void finish_kernel(const double *__restrict__ A, double *__restrict__ pk, int n)
+{
+    long long no2 = (long long)n * (n + 1) / 2;
+    for (long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x; ij < no2;
+         ij += (long long)gridDim.x * blockDim.x) {
+        // invert ij = i(i+1)/2 + j
+        int i = (int)((sqrt(8.0 * (double)ij + 1.0) - 1.0) * 0.5);
+        while ((long long)(i + 1) * (i + 2) / 2 <= ij) ++i;
+        while ((long long)i * (i + 1) / 2 > ij) --i;
+        int j = (int)(ij - (long long)i * (i + 1) / 2);
+        pk[ij] = A[(size_t)i * n + j] + A[(size_t)j * n + i];
+    }
+}
+
+// Independent FMA chains: 8 per thread, `iters` steps each.
+__global__ void fma_probe_kernel(double *out, int iters, double a, double b)
+{
+    double x0 = threadIdx.x * 1e-9, x1 = x0 + 0.1, x2 = x0 + 0.2, x3 = x0 + 0.3;
+    double x4 = x0 + 0.4, x5 = x0 + 0.5, x6 = x0 + 0.6, x7 = x0 + 0.7;
+    for (int i = 0; i < iters; ++i) {
+        x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+        x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+    const double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1234.5678) out[0] = s;   // keeps the chains alive
+}
+
+static int grid_for(long long work, int num_sms)
+{
+    long long b = (work + 255) / 256;
+    long long cap = (long long)num_sms * 8;
+    return (int)std::max<long long>(1, std::min(b, cap));
+}
+
+static int launch_fock(patgpu_basis *h, int mode, cudaStream_t s)
+{
+    EriArgs a = h->base_args();
+    a.mode = mode;
+    a.D0 = h->d_D0.as<double>();
+    a.D1 = h->d_D1.as<double>();
+    a.A0 = h->d_A0.as<double>();
+    a.A1 = h->d_A1.as<double>();
+    PG_CUDA(cudaEventRecord(h->ev0, s));
+    int launches = 0;
+    for (auto &w : h->work) {
+        a.quart = h->d_quart.as<int2>() + w.offset;
+        a.nquart = w.count;
+        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms));
+        ++launches;
+    }
+    PG_CUDA(cudaEventRecord(h->ev1, s));
+    h->last_launches = launches;
+    return 0;
+}
+
+static int ensure_work(patgpu_basis *h, bool two)
+{
+    const size_t nn = (size_t)h->n * h->n, no2 = (size_t)h->n * (h->n + 1) / 2;
+    PG_CUDA(h->d_D0.ensure(sizeof(double) * nn));
+    PG_CUDA(h->d_A0.ensure(sizeof(double) * nn));
+    PG_CUDA(h->d_Pk0.ensure(sizeof(double) * no2));
+    PG_CUDA(h->d_Gk0.ensure(sizeof(double) * no2));
+    if (two) {
+        PG_CUDA(h->d_D1.ensure(sizeof(double) * nn));
+        PG_CUDA(h->d_A1.ensure(sizeof(double) * nn));
+        PG_CUDA(h->d_Pk1.ensure(sizeof(double) * no2));
+        PG_CUDA(h->d_Gk1.ensure(sizeof(double) * no2));
+    }
+    return 0;
+}
+
+static int record_timing(patgpu_basis *h)
+{
+    float ms = 0.f;
+    PG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->last_ns = ms * 1e6;
+    return 0;
+}
+
+// Host-buffer Fock build shared by the RHF / UHF / JK entry points.
+static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *P1, double *G0, double *G1)
+{
+    if (!h) return fail(PATGPU_EINVAL, "null handle");
+    const bool two = mode != MODE_RHF;
+    int rc = ensure_work(h, two);
+    if (rc) return rc;
+    const size_t nn = (size_t)h->n * h->n, no2 = (size_t)h->n * (h->n + 1) / 2;
+    cudaStream_t s = h->stream;
+    const int g = grid_for((long long)nn, h->num_sms);
+    PG_CUDA(cudaMemcpyAsync(h->d_Pk0.p, P0, sizeof(double) * no2, cudaMemcpyHostToDevice, s));
+    unpack_kernel<<<g, 256, 0, s>>>(h->d_Pk0.as<double>(), h->d_D0.as<double>(), h->n);
+    if (mode == MODE_UHF) {
+        PG_CUDA(cudaMemcpyAsync(h->d_Pk1.p, P1, sizeof(double) * no2, cudaMemcpyHostToDevice, s));
+        unpack_kernel<<<g, 256, 0, s>>>(h->d_Pk1.as<double>(), h->d_D1.as<double>(), h->n);
+    }
+    PG_CUDA(cudaMemsetAsync(h->d_A0.p, 0, sizeof(double) * nn, s));
+    if (two) PG_CUDA(cudaMemsetAsync(h->d_A1.p, 0, sizeof(double) * nn, s));
+    rc = launch_fock(h, mode, s);
+    if (rc) return rc;
+    finish_kernel<<<grid_for((long long)no2, h->num_sms), 256, 0, s>>>(h->d_A0.as<double>(), h->d_Gk0.as<double>(),
+                                                                      h->n);
+    if (two)
+        finish_kernel<<<grid_for((long long)no2, h->num_sms), 256, 0, s>>>(h->d_A1.as<double>(),
+                                                                          h->d_Gk1.as<double>(), h->n);
+    PG_CUDA(cudaGetLastError());
+    h->h_stage.resize(2 * no2);
+    PG_CUDA(cudaMemcpyAsync(h->h_stage.data(), h->d_Gk0.p, sizeof(double) * no2, cudaMemcpyDeviceToHost, s));
+    if (two)
+        PG_CUDA(cudaMemcpyAsync(h->h_stage.data() + no2, h->d_Gk1.p, sizeof(double) * no2, cudaMemcpyDeviceToHost,
+                                s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    rc = record_timing(h);
+    if (rc) return rc;
+    for (size_t i = 0; i < no2; ++i) G0[i] += h->h_stage[i];
+    if (two)
+        for (size_t i = 0; i < no2; ++i) G1[i] += h->h_stage[no2 + i];
+    return 0;
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+// =================================================================== C ABI
+extern "C" {
+
+int patgpu_last_error(void) { return pg::t_err; }
+const char *patgpu_error_message(void) { return pg::t_msg; }
+
+int patgpu_rys_host(int n, double T, double *x, double *w)
+{
+    if (n < 1 || n > RYS_NMAX || !(T >= 0.0) || !x || !w) return fail(PATGPU_EINVAL, "bad Rys request");
+    static RysConst rc = host_rys_const();
+    for (int f = 0; f < n; ++f) {
+        x[f] = rys_eval(n, f, T, rc, rys_coef_host, RYS_DEG);
+        w[f] = rys_eval(n, n + f, T, rc, rys_coef_host, RYS_DEG);
+    }
+    return 0;
+}
+
+int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off, const int *nst,
+                        const int *prim_off, const double *alpha, const double *coef, int ncen,
+                        const double *charge, const double *xyz, int skipcen, double schwarz_tau,
+                        patgpu_handle *out)
+{
+    if (!out || nshell < 1 || ncen < 1 || !l || !cen || !off || !nst || !prim_off || !alpha || !coef || !charge ||
+        !xyz)
+        return fail(PATGPU_EINVAL, "patgpu_basis_create: null or empty argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(PATGPU_ENODEV, "no CUDA device: the GPU library has no CPU path");
+    int n = 0;
+    for (int s = 0; s < nshell; ++s) {
+        if (nst[s] && (l[s] < 0 || l[s] > PG_LMAX))
+            return fail(PATGPU_EUNSUPPORTED, "shell %d has l = %d; the kernels support l <= %d", s, l[s], PG_LMAX);
+        if (nst[s] && nst[s] != ncart(l[s])) return fail(PATGPU_EINVAL, "shell %d: nst %d != ncart(%d)", s, nst[s], l[s]);
+        if (cen[s] < 0 || cen[s] >= ncen) return fail(PATGPU_EINVAL, "shell %d: bad centre %d", s, cen[s]);
+        if (prim_off[s + 1] <= prim_off[s]) return fail(PATGPU_EINVAL, "shell %d has no primitives", s);
+        if (nst[s]) n = std::max(n, off[s] + nst[s]);
+    }
+    if (n < 1) return fail(PATGPU_EINVAL, "basis has no functions");
+    int rc = init_tables();
+    if (rc) return rc;
+    patgpu_basis *h = new patgpu_basis();
+    h->nsh = nshell;
+    h->ncen = ncen;
+    h->n = n;
+    h->skipcen = skipcen;
+    h->tau = schwarz_tau;
+    h->l.assign(l, l + nshell);
+    h->cen.assign(cen, cen + nshell);
+    h->off.assign(off, off + nshell);
+    h->nst.assign(nst, nst + nshell);
+    h->poff.assign(prim_off, prim_off + nshell + 1);
+    h->al.assign(alpha, alpha + prim_off[nshell]);
+    h->co.assign(coef, coef + prim_off[nshell]);
+    h->q.assign(charge, charge + ncen);
+    h->xyz.assign(xyz, xyz + 3 * ncen);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
+        h->d_err.ensure(sizeof(int)) != cudaSuccess) {
+        delete h;
+        return fail(PATGPU_ECUDA, "stream/event creation failed");
+    }
+    cudaMemset(h->d_err.p, 0, sizeof(int));
+    rc = build_pairs(h);
+    if (!rc) rc = build_schwarz(h);
+    if (!rc) rc = build_quartets(h);
+    if (rc) {
+        patgpu_basis_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+int patgpu_basis_destroy(patgpu_handle h)
+{
+    if (!h) return 0;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return 0;
+}
+
+int patgpu_set_quartets(patgpu_handle h, int start_shell, int rank, int nranks)
+{
+    if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(PATGPU_EINVAL, "bad partition");
+    h->start_shell = start_shell;
+    h->rank = rank;
+    h->nranks = nranks;
+    return build_quartets(h);
+}
+
+int patgpu_rhf_gmatrix(patgpu_handle h, const double *P, double *G)
+{
+    if (!P || !G) return fail(PATGPU_EINVAL, "null matrix");
+    return host_fock(h, MODE_RHF, P, nullptr, G, nullptr);
+}
+
+int patgpu_uhf_gmatrix(patgpu_handle h, const double *PA, const double *PB, double *GA, double *GB)
+{
+    if (!PA || !PB || !GA || !GB) return fail(PATGPU_EINVAL, "null matrix");
+    return host_fock(h, MODE_UHF, PA, PB, GA, GB);
+}
+
+int patgpu_jk(patgpu_handle h, const double *P, double *J, double *K)
+{
+    if (!P || !J || !K) return fail(PATGPU_EINVAL, "null matrix");
+    return host_fock(h, MODE_JK, P, nullptr, J, K);
+}
+
+int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, void *stream)
+{
+    if (!h || !dP || !dA) return fail(PATGPU_EINVAL, "null argument");
+    int rc = ensure_work(h, false);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nn = (size_t)h->n * h->n;
+    unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(dP, h->d_D0.as<double>(), h->n);
+    PG_CUDA(cudaMemsetAsync(dA, 0, sizeof(double) * nn, s));
+    EriArgs a = h->base_args();
+    a.mode = MODE_RHF;
+    a.D0 = h->d_D0.as<double>();
+    a.A0 = dA;
+    PG_CUDA(cudaEventRecord(h->ev0, s));
+    int launches = 0;
+    for (auto &w : h->work) {
+        a.quart = h->d_quart.as<int2>() + w.offset;
+        a.nquart = w.count;
+        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms));
+        ++launches;
+    }
+    PG_CUDA(cudaEventRecord(h->ev1, s));
+    h->last_launches = launches;
+    return 0;
+}
+
+int patgpu_finish_gmatrix_device(patgpu_handle h, const double *dA, double *dG, void *stream)
+{
+    if (!h || !dA || !dG) return fail(PATGPU_EINVAL, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long no2 = (long long)h->n * (h->n + 1) / 2;
+    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(dA, dG, h->n);
+    PG_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, void *stream)
+{
+    if (!h) return fail(PATGPU_EINVAL, "null handle");
+    int rc = ensure_work(h, false);
+    if (rc) return rc;
+    rc = patgpu_rhf_accumulate_device(h, dP, h->d_A0.as<double>(), stream);
+    if (rc) return rc;
+    return patgpu_finish_gmatrix_device(h, h->d_A0.as<double>(), dG, stream);
+}
+
+int patgpu_eri_quartets(patgpu_handle h, int nq, const int *sh4, double *out)
+{
+    if (!h || nq < 0 || (nq && (!sh4 || !out))) return fail(PATGPU_EINVAL, "bad arguments");
+    // (shell i, shell j) -> pair index
+    std::vector<int> pidx((size_t)h->nsh * h->nsh, -1);
+    for (int u = 0; u < h->npair; ++u) {
+        pidx[(size_t)h->psa[u] * h->nsh + h->psb[u]] = u;
+        pidx[(size_t)h->psb[u] * h->nsh + h->psa[u]] = u;
+    }
+    std::vector<int2> qs(nq);
+    std::vector<char> swapbk(nq);
+    for (int k = 0; k < nq; ++k) {
+        const int *s = sh4 + 4 * k;
+        for (int t = 0; t < 4; ++t)
+            if (s[t] < 0 || s[t] >= h->nsh || !h->nst[s[t]]) return fail(PATGPU_EINVAL, "quartet %d: bad shell", k);
+        int u = pidx[(size_t)s[0] * h->nsh + s[1]], v = pidx[(size_t)s[2] * h->nsh + s[3]];
+        swapbk[k] = h->pcls[u] < h->pcls[v] || (h->pcls[u] == h->pcls[v] && u < v);
+        qs[k] = swapbk[k] ? make_int2(v, u) : make_int2(u, v);
+    }
+    std::vector<double> buf;
+    std::vector<long long> offs;
+    int rc = export_pairs(h, qs, buf, offs);
+    if (rc) return rc;
+    size_t o = 0;
+    for (int k = 0; k < nq; ++k) {
+        const int *s = sh4 + 4 * k;
+        const int n0 = h->nst[s[0]], n1 = h->nst[s[1]], n2 = h->nst[s[2]], n3 = h->nst[s[3]];
+        // kernel orientation: bra pair (x,y) with x the first shell of the pair
+        const int u = qs[k].x, v = qs[k].y;
+        const int bx = h->psa[u], kx = h->psa[v];
+        const int nby = h->nst[h->psb[u]];
+        const int nkx = h->nst[h->psa[v]], nky = h->nst[h->psb[v]];
+        const double *blk = buf.data() + offs[k];
+        for (int i0 = 0; i0 < n0; ++i0)
+            for (int i1 = 0; i1 < n1; ++i1)
+                for (int i2 = 0; i2 < n2; ++i2)
+                    for (int i3 = 0; i3 < n3; ++i3) {
+                        // requested (s0 s1 | s2 s3); kernel (bx by | kx ky) possibly bra/ket swapped
+                        int c01[2] = {i0, i1}, c23[2] = {i2, i3};
+                        int *cb = swapbk[k] ? c23 : c01, *ck = swapbk[k] ? c01 : c23;
+                        const int *sb = swapbk[k] ? s + 2 : s, *skt = swapbk[k] ? s : s + 2;
+                        int ibx = (sb[0] == bx) ? cb[0] : cb[1];
+                        int iby = (sb[0] == bx) ? cb[1] : cb[0];
+                        int ikx = (skt[0] == kx) ? ck[0] : ck[1];
+                        int iky = (skt[0] == kx) ? ck[1] : ck[0];
+                        out[o++] = blk[(((size_t)ibx * nby + iby) * nkx + ikx) * nky + iky];
+                    }
+    }
+    return 0;
+}
+
+int patgpu_select_device(int index)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(PATGPU_ENODEV, "no CUDA device");
+    PG_CUDA(cudaSetDevice(((index % ndev) + ndev) % ndev));
+    return 0;
+}
+
+int patgpu_fp64_peak(double *tflops)
+{
+    if (!tflops) return fail(PATGPU_EINVAL, "null argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(PATGPU_ENODEV, "no CUDA device");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    DBuf out;
+    PG_CUDA(out.ensure(sizeof(double)));
+    cudaEvent_t e0, e1;
+    PG_CUDA(cudaEventCreate(&e0));
+    PG_CUDA(cudaEventCreate(&e1));
+    const int iters = 1 << 15, threads = 256, blocks = sms * 8;
+    fma_probe_kernel<<<blocks, threads>>>(out.as<double>(), iters, 0.999999999, 1e-9);   // warm-up
+    PG_CUDA(cudaEventRecord(e0));
+    for (int r = 0; r < 4; ++r) fma_probe_kernel<<<blocks, threads>>>(out.as<double>(), iters, 0.999999999, 1e-9);
+    PG_CUDA(cudaEventRecord(e1));
+    PG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *tflops = 4.0 * 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+    return 0;
+}
+
+int patgpu_stats(patgpu_handle h, long long *o)
+{
+    if (!h || !o) return fail(PATGPU_EINVAL, "null argument");
+    o[0] = h->n;
+    o[1] = h->npair;
+    o[2] = h->nquart;
+    o[3] = (long long)h->work.size();
+    o[4] = h->nquart_unscreened;
+    return 0;
+}
+
+int patgpu_class_counts(patgpu_handle h, int max, int *l4, long long *counts)
+{
+    if (!h || !l4 || !counts) return fail(PATGPU_EINVAL, "null argument");
+    int k = 0;
+    for (auto &w : h->work) {
+        if (k >= max) break;
+        l4[4 * k] = w.la; l4[4 * k + 1] = w.lb; l4[4 * k + 2] = w.lc; l4[4 * k + 3] = w.ld;
+        counts[k] = w.count;
+        ++k;
+    }
+    return k;
+}
+
+int patgpu_last_timing(patgpu_handle h, double *ns, int *launches)
+{
+    if (!h) return fail(PATGPU_EINVAL, "null handle");
+    if (ns) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last_ns = ms * 1e6;
+        *ns = h->last_ns;
+    }
+    if (launches) *launches = h->last_launches;
+    return 0;
+}
+
+int patgpu_oneints(patgpu_handle h, double *S, double *T, double *H)
+{
+    if (!h || !S || !T || !H) return fail(PATGPU_EINVAL, "null argument");
+    return run_oneints(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
+                       h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n, S, T, H,
+                       nullptr, h->stream);
+}
+
+int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, const int *nst,
+                   const int *prim_off, const double *alpha, const double *coef, int ncen,
+                   const double *charge, const double *xyz, int skipcen, double *S, double *T,
+                   double *H, double *Hdpm)
+{
+    if (nshell < 1 || !l || !cen || !off || !nst || !prim_off || !alpha || !coef || !charge || !xyz)
+        return fail(PATGPU_EINVAL, "patgpu_onebody: null argument");
+    if ((S || T || H) && !(S && T && H)) return fail(PATGPU_EINVAL, "patgpu_onebody: S, T, H go together");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(PATGPU_ENODEV, "no CUDA device: the GPU library has no CPU path");
+    int n = 0;
+    for (int s = 0; s < nshell; ++s) {
+        if (nst[s] && (l[s] < 0 || l[s] > PG_LMAX))
+            return fail(PATGPU_EUNSUPPORTED, "shell %d has l = %d; the kernels support l <= %d", s, l[s], PG_LMAX);
+        if (nst[s]) n = std::max(n, off[s] + nst[s]);
+    }
+    int rc = init_tables();
+    if (rc) return rc;
+    return run_oneints(nshell, l, cen, off, nst, prim_off, alpha, coef, ncen, charge, xyz, skipcen, n, S, T, H, Hdpm,
+                       nullptr);
+}
+
+int patgpu_dpm(patgpu_handle h, double *H)
+{
+    if (!h || !H) return fail(PATGPU_EINVAL, "null argument");
+    return run_oneints(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
+                       h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n, nullptr,
+                       nullptr, nullptr, H, h->stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,20 @@
+// onebody.cuh -- McMurchie-Davidson one-body integrals: overlap, kinetic,
+// nuclear attraction and the distributed-positron-model potential.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace pg {
+
+cudaError_t upload_onebody_constants();
+
+// If S, T, H are non-null they are overwritten with the packed S, T and
+// H = T + V (V over every centre but skipcen, oneints.c:139-234).  If Hdpm
+// is non-null, Hdpm -= V_DPM (dpmints.c:121-199).  Host buffers; returns 0
+// or a PATGPU_E* code.
+int run_oneints(int nsh, const int *l, const int *cen, const int *off, const int *nst, const int *poff,
+                const double *al, const double *co, int ncen, const double *q, const double *xyz, int skipcen,
+                int n, double *S, double *T, double *H, double *Hdpm, cudaStream_t stream);
+
+int fail(int code, const char *fmt, ...);
+
+}  // namespace pg

@@ -1,0 +1,217 @@
+"""Python host mirror of the reference's integral / Fock-build interface over
+the C ABI of libpatgpu.so (include/patgpu.h).
+
+The class ``GpuBasis`` plays the role of the reference's basis module plus
+ERIFS handle: ``two_electron_ints`` builds the screened quartet list,
+``rhf_form_gmatrix`` / ``uhf_form_gmatrix`` accumulate G into packed lower
+triangles exactly like scfaux.c:429-714, ``dpm_ints`` subtracts the DPM
+potential (dpmints.c:121-199) and ``one_electron_ints`` fills S, T, H
+(oneints.c:139-234).  Failures raise ``PatgpuError``; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpatgpu.so")
+
+_lib = None
+
+
+class PatgpuError(RuntimeError):
+    pass
+
+
+def build(force: bool = False) -> str:
+    """Compile libpatgpu.so for sm_100a (nvcc; no GPU needed)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc")], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PatgpuError(f"{LIB_PATH} is missing: build it with `make -C patmol_b200/csrc`")
+        L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lp = ctypes.POINTER(ctypes.c_longlong)
+        H = ctypes.c_void_p
+        L.patgpu_last_error.restype = ctypes.c_int
+        L.patgpu_error_message.restype = ctypes.c_char_p
+        L.patgpu_basis_create.argtypes = [ctypes.c_int, ip, ip, ip, ip, ip, dp, dp, ctypes.c_int, dp, dp,
+                                          ctypes.c_int, ctypes.c_double, ctypes.POINTER(H)]
+        L.patgpu_basis_destroy.argtypes = [H]
+        L.patgpu_set_quartets.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.patgpu_rhf_gmatrix.argtypes = [H, dp, dp]
+        L.patgpu_uhf_gmatrix.argtypes = [H, dp, dp, dp, dp]
+        L.patgpu_jk.argtypes = [H, dp, dp, dp]
+        L.patgpu_rhf_gmatrix_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.patgpu_rhf_accumulate_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.patgpu_finish_gmatrix_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.patgpu_eri_quartets.argtypes = [H, ctypes.c_int, ip, dp]
+        L.patgpu_oneints.argtypes = [H, dp, dp, dp]
+        L.patgpu_dpm.argtypes = [H, dp]
+        L.patgpu_onebody.argtypes = [ctypes.c_int, ip, ip, ip, ip, ip, dp, dp, ctypes.c_int, dp, dp, ctypes.c_int,
+                                     dp, dp, dp, dp]
+        L.patgpu_stats.argtypes = [H, lp]
+        L.patgpu_class_counts.argtypes = [H, ctypes.c_int, ip, lp]
+        L.patgpu_last_timing.argtypes = [H, dp, ip]
+        L.patgpu_rys_host.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
+        L.patgpu_fp64_peak.argtypes = [dp]
+        _lib = L
+    return _lib
+
+
+def _p(a, t=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = lib().patgpu_error_message().decode(errors="replace")
+        raise PatgpuError(f"{what}: {msg} (code {rc})")
+
+
+def fp64_peak_tflops() -> float:
+    v = ctypes.c_double()
+    _check(lib().patgpu_fp64_peak(ctypes.byref(v)), "patgpu_fp64_peak")
+    return v.value
+
+
+def rys_host(n: int, T: float):
+    """Nodes (t^2) and weights of the tables the kernels use, evaluated on the host."""
+    x = np.zeros(n)
+    w = np.zeros(n)
+    _check(lib().patgpu_rys_host(n, float(T), _p(x), _p(w)), "patgpu_rys_host")
+    return x, w
+
+
+class GpuBasis:
+    """A basis bound to the current CUDA device (see patgpu_basis_create)."""
+
+    def __init__(self, basis, schwarz_tau: float = 1e-14):
+        self.basis = basis
+        self.n = basis.norb
+        self.no2 = self.n * (self.n + 1) // 2
+        self._f = basis.flat_arrays()
+        f = self._f
+        h = ctypes.c_void_p()
+        _check(lib().patgpu_basis_create(basis.nshell, _p(f["l"], ctypes.c_int), _p(f["cen"], ctypes.c_int),
+                                         _p(f["off"], ctypes.c_int), _p(f["nst"], ctypes.c_int),
+                                         _p(f["prim_off"], ctypes.c_int), _p(f["alpha"]), _p(f["coef"]),
+                                         basis.ncen, _p(f["charges"]), _p(f["coords"]), basis.skipcen,
+                                         float(schwarz_tau), ctypes.byref(h)), "patgpu_basis_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().patgpu_basis_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference-shaped interface -------------------------------------
+    def two_electron_ints(self, start: int = 0, rank: int = 0, nranks: int = 1):
+        _check(lib().patgpu_set_quartets(self.h, start, rank, nranks), "two_electron_ints")
+
+    def rhf_form_gmatrix(self, P, G=None):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        G = np.zeros(self.no2) if G is None else G
+        _check(lib().patgpu_rhf_gmatrix(self.h, _p(P), _p(G)), "rhf_form_gmatrix")
+        return G
+
+    def uhf_form_gmatrix(self, PA, PB, GA=None, GB=None):
+        PA = np.ascontiguousarray(PA, dtype=np.float64)
+        PB = np.ascontiguousarray(PB, dtype=np.float64)
+        GA = np.zeros(self.no2) if GA is None else GA
+        GB = np.zeros(self.no2) if GB is None else GB
+        _check(lib().patgpu_uhf_gmatrix(self.h, _p(PA), _p(PB), _p(GA), _p(GB)), "uhf_form_gmatrix")
+        return GA, GB
+
+    def jk(self, P):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        J = np.zeros(self.no2)
+        K = np.zeros(self.no2)
+        _check(lib().patgpu_jk(self.h, _p(P), _p(J), _p(K)), "patgpu_jk")
+        return J, K
+
+    def one_electron_ints(self):
+        S, T, H = np.zeros(self.no2), np.zeros(self.no2), np.zeros(self.no2)
+        _check(lib().patgpu_oneints(self.h, _p(S), _p(T), _p(H)), "one_electron_ints")
+        return S, T, H
+
+    def dpm_ints(self, H):
+        H = np.array(H, dtype=np.float64)
+        _check(lib().patgpu_dpm(self.h, _p(H)), "dpm_ints")
+        return H
+
+    # -- extras -----------------------------------------------------------
+    def eri_quartets(self, quartets):
+        q = np.ascontiguousarray(np.asarray(quartets, dtype=np.int32).reshape(-1, 4))
+        sh = self.basis.shells
+        sizes = [sh[a].nst * sh[b].nst * sh[c].nst * sh[d].nst for a, b, c, d in q]
+        out = np.zeros(int(sum(sizes)))
+        _check(lib().patgpu_eri_quartets(self.h, len(q), _p(q, ctypes.c_int), _p(out)), "patgpu_eri_quartets")
+        blocks, o = [], 0
+        for (a, b, c, d), s in zip(q, sizes):
+            blocks.append(out[o:o + s].reshape(sh[a].nst, sh[b].nst, sh[c].nst, sh[d].nst))
+            o += s
+        return blocks
+
+    def rhf_gmatrix_device(self, dP_ptr: int, dG_ptr: int, stream: int):
+        """stream: the raw cudaStream_t handle (e.g. torch.cuda.Stream.cuda_stream)."""
+        _check(lib().patgpu_rhf_gmatrix_device(self.h, dP_ptr, dG_ptr, stream), "rhf_gmatrix_device")
+
+    def rhf_accumulate_device(self, dP_ptr: int, dA_ptr: int, stream: int):
+        _check(lib().patgpu_rhf_accumulate_device(self.h, dP_ptr, dA_ptr, stream), "accumulate")
+
+    def finish_gmatrix_device(self, dA_ptr: int, dG_ptr: int, stream: int):
+        _check(lib().patgpu_finish_gmatrix_device(self.h, dA_ptr, dG_ptr, stream), "finish")
+
+    def stats(self):
+        o = np.zeros(5, dtype=np.int64)
+        _check(lib().patgpu_stats(self.h, _p(o, ctypes.c_longlong)), "patgpu_stats")
+        return dict(n=int(o[0]), pairs=int(o[1]), quartets=int(o[2]), classes=int(o[3]), unscreened=int(o[4]))
+
+    def class_counts(self):
+        l4 = np.zeros(4 * 128, dtype=np.int32)
+        c = np.zeros(128, dtype=np.int64)
+        k = lib().patgpu_class_counts(self.h, 128, _p(l4, ctypes.c_int), _p(c, ctypes.c_longlong))
+        return [(tuple(int(v) for v in l4[4 * i:4 * i + 4]), int(c[i])) for i in range(k)]
+
+    def last_timing(self):
+        ns = ctypes.c_double()
+        n = ctypes.c_int()
+        _check(lib().patgpu_last_timing(self.h, ctypes.byref(ns), ctypes.byref(n)), "patgpu_last_timing")
+        return ns.value, n.value
+
+
+def onebody(basis, want_sth=True, Hdpm=None):
+    """Handle-free one-body integrals (patgpu_onebody)."""
+    f = basis.flat_arrays()
+    no2 = basis.norb * (basis.norb + 1) // 2
+    S = T = H = None
+    null = ctypes.POINTER(ctypes.c_double)()
+    if want_sth:
+        S, T, H = np.zeros(no2), np.zeros(no2), np.zeros(no2)
+    if Hdpm is not None:
+        Hdpm = np.array(Hdpm, dtype=np.float64)
+    _check(lib().patgpu_onebody(basis.nshell, _p(f["l"], ctypes.c_int), _p(f["cen"], ctypes.c_int),
+                                _p(f["off"], ctypes.c_int), _p(f["nst"], ctypes.c_int),
+                                _p(f["prim_off"], ctypes.c_int), _p(f["alpha"]), _p(f["coef"]), basis.ncen,
+                                _p(f["charges"]), _p(f["coords"]), basis.skipcen,
+                                _p(S) if want_sth else null, _p(T) if want_sth else null,
+                                _p(H) if want_sth else null, _p(Hdpm) if Hdpm is not None else null),
+           "patgpu_onebody")
+    return S, T, H, Hdpm

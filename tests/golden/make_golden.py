@@ -80,7 +80,16 @@ def main():
     scf = json.loads(out.strip().splitlines()[-1])
     np.savez_compressed(os.path.join(OUT, "water_spd.npz"), G=g["G.bin"], GA=u["GA.bin"], GB=u["GB.bin"],
                         S=s["S.bin"], T=s["T.bin"], H=s["H.bin"], Pconv=c["Pconv.bin"])
-    meta["water_spd"] = {"P_seed": 11, "PB_seed": 12, "scf": scf, "nrec": int(s["info.txt"].split()[4])}
+    # first-order energy of exact integrals at the reference's converged
+    # density: E + tr(P dG), dG = G_exact(P) - G_reference(P); the SCF energy
+    # is stationary in P, so this is the exact-integral energy to second order
+    Pc = c["Pconv.bin"]
+    _, gc = patref.run_ref(b, ["gmat", "P.bin"], inputs={"P.bin": Pc}, outputs=["G.bin"])
+    dG = patref.Oracle(b).gmat(Pc) - gc["G.bin"]
+    from patmol_b200.basis import unpack
+    de = float(np.sum(unpack(Pc, n) * unpack(dG, n)))
+    meta["water_spd"] = {"P_seed": 11, "PB_seed": 12, "scf": scf, "nrec": int(s["info.txt"].split()[4]),
+                         "e_total_exact_integrals": scf["e_total"] + de, "de_root_defect": de}
 
     # 3. He + DPM regression (positron at (0,0,3) bohr)
     b = he_dpm_basis()
