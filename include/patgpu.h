@@ -118,6 +118,23 @@ int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, voi
 int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, void *stream);
 int patgpu_finish_gmatrix_device(patgpu_handle h, const double *dA, double *dG, void *stream);
 
+/* No counterpart in the reference.  The same device-resident RHF Fock build
+ * as patgpu_rhf_gmatrix_device, for callers that must not allocate GPU
+ * memory once they are running: a solver embedded in a host program that
+ * owns all device memory through its own pool, or code on a path where a
+ * cudaMalloc would synchronise the device or fail.  Its two n x n working
+ * matrices live in a fixed 4 MiB array compiled into the library (every
+ * GPU that loads the library holds it until the process exits), so the
+ * basis must have at most 512 functions; larger bases are rejected with
+ * PATGPU_EINVAL.  The handle itself is built beforehand by
+ * patgpu_basis_create, which does allocate.  The first call on a device
+ * looks up the array's device address there, so make that first call before
+ * any stream capture.  All calls share the one array: calls that overlap on
+ * the GPU (different streams, or different handles on one device at the
+ * same time) race and give wrong G.  dP, dG and stream as for
+ * patgpu_rhf_gmatrix_device; dG is overwritten. */
+int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double *dG, void *stream);
+
 /* Integrals of arbitrary shell quartets (a b | c d), nq x 4 shell indices;
  * out receives, per quartet in order, na*nb*nc*nd values indexed
  * ((ia nb + ib) nc + ic) nd + id with the reference's component order and

@@ -656,6 +656,79 @@ int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, voi
     return patgpu_finish_gmatrix_device(h, h->d_A0.as<double>(), dG, stream);
 }
 
+// ------------------------------------------------ allocation-free build
+// patgpu_rhf_gmatrix_device_noalloc keeps its working matrices (the full
+// density and the unsymmetrised accumulator, n*n doubles each) in this
+// fixed array instead of buffers obtained from cudaMalloc.  It is sized for
+// n <= kNoAllocMaxN basis functions: 2 * 512 * 512 doubles = 4 MiB, held by
+// every GPU that loads the library until the process exits.  Host code may
+// not use the array's name as a device address; the address is looked up
+// per device with cudaGetSymbolAddress the first time the entry point runs
+// on that device.
+}  // extern "C"
+namespace pg {
+constexpr int kNoAllocMaxN = 512;
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxN * kNoAllocMaxN];
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_lock;
+static double *g_noalloc_ptr[kNoAllocMaxDevices];
+
+static int noalloc_scratch(double **out)
+{
+    int dev = 0;
+    PG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(PATGPU_EINVAL, "device %d is beyond the %d devices the fixed scratch tracks", dev,
+                    kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> g(g_noalloc_lock);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(PATGPU_ECUDA, "cudaGetSymbolAddress of the fixed scratch failed on device %d: %s", dev,
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return 0;
+}
+}  // namespace pg
+extern "C" {
+
+int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double *dG, void *stream)
+{
+    if (!h || !dP || !dG) return fail(PATGPU_EINVAL, "null argument");
+    if (h->n > kNoAllocMaxN)
+        return fail(PATGPU_EINVAL,
+                    "patgpu_rhf_gmatrix_device_noalloc: the basis has %d functions but its fixed scratch holds "
+                    "at most %d; use patgpu_rhf_gmatrix_device",
+                    h->n, kNoAllocMaxN);
+    double *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    const int n = h->n;
+    const size_t nn = (size_t)n * n;
+    double *D = scratch, *A = scratch + nn;
+    cudaStream_t s = (cudaStream_t)stream;
+    // D is fully rewritten; A keeps the previous call's sums and must start at zero
+    unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(dP, D, n);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * nn, s));
+    EriArgs a = h->base_args();
+    a.mode = MODE_RHF;
+    a.D0 = D;
+    a.A0 = A;
+    for (auto &w : h->work) {
+        a.quart = h->d_quart.as<int2>() + w.offset;
+        a.nquart = w.count;
+        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms));
+    }
+    const long long no2 = (long long)n * (n + 1) / 2;
+    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(A, dG, n);
+    PG_CUDA(cudaGetLastError());
+    return 0;
+}
+
 int patgpu_eri_quartets(patgpu_handle h, int nq, const int *sh4, double *out)
 {
     if (!h || nq < 0 || (nq && (!sh4 || !out))) return fail(PATGPU_EINVAL, "bad arguments");

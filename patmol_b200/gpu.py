@@ -55,6 +55,7 @@ def lib():
         L.patgpu_rhf_gmatrix_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.patgpu_rhf_accumulate_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.patgpu_finish_gmatrix_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.patgpu_rhf_gmatrix_device_noalloc.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.patgpu_eri_quartets.argtypes = [H, ctypes.c_int, ip, dp]
         L.patgpu_oneints.argtypes = [H, dp, dp, dp]
         L.patgpu_dpm.argtypes = [H, dp]
@@ -172,6 +173,12 @@ class GpuBasis:
     def rhf_gmatrix_device(self, dP_ptr: int, dG_ptr: int, stream: int):
         """stream: the raw cudaStream_t handle (e.g. torch.cuda.Stream.cuda_stream)."""
         _check(lib().patgpu_rhf_gmatrix_device(self.h, dP_ptr, dG_ptr, stream), "rhf_gmatrix_device")
+
+    def rhf_gmatrix_device_noalloc(self, dP_ptr: int, dG_ptr: int, stream: int):
+        """Same result as rhf_gmatrix_device without any device allocation
+        (working matrices in the library's fixed scratch; n <= 512)."""
+        _check(lib().patgpu_rhf_gmatrix_device_noalloc(self.h, dP_ptr, dG_ptr, stream),
+               "rhf_gmatrix_device_noalloc")
 
     def rhf_accumulate_device(self, dP_ptr: int, dA_ptr: int, stream: int):
         _check(lib().patgpu_rhf_accumulate_device(self.h, dP_ptr, dA_ptr, stream), "accumulate")
