@@ -1,33 +1,10 @@
-// eri.cu -- two-electron integrals over contracted Cartesian shell quartets
-// by Rys quadrature, fused with their digestion into the Coulomb/exchange
-// (G) matrices, one kernel instantiation per angular-momentum class.
-//
-// Algorithm (the same mathematics as twoints.c:23-186 and rys.c:2269-2336):
-//   per primitive quartet: p, q, P, Q, T = pq/(p+q)|PQ|^2, n = L/2+1 Rys
-//   nodes x_r = t_r^2 and weights w_r; per node and Cartesian direction the
-//   2-D recursion G[i][j] (i <= la+lb, j <= lc+ld) from B00, B10, B01, C00,
-//   C00'; the binomial transfer to I[a][b][c][d]; the integral of a
-//   component quartet is sum_r Ix Iy Iz with w_r and the prefactor
-//   2 pi^{5/2} K_ab K_cd / sqrt(p+q) folded into the z factor.
-//
-// GPU mapping: a team of TQ threads owns one shell quartet (TQ = 1 for the
-// small classes, up to 128 for (ff|ff)).  Within the team the lanes split
-// the root/weight evaluation (one Chebyshev series each), the (root,
-// direction) recursions, the component integrals and finally the digestion
-// targets.  The per-quartet tables and integrals live in shared memory;
-// the block's teams advance in lock step, separated by block barriers.
-//
-// Digestion (8-fold symmetry with a degeneracy factor instead of the
-// reference's per-integral index tests, scfaux.c:446-495): with deg = 8 /
-// |symmetry group of the shell quartet| and every component integral v of
-// the block,
-//     Jacc(f1,f2) += deg v D(f3,f4)    Jacc(f3,f4) += deg v D(f1,f2)
-//     Kacc(f1,f3) += deg v D(f2,f4)    Kacc(f2,f4) += deg v D(f1,f3)
-//     Kacc(f1,f4) += deg v D(f2,f3)    Kacc(f2,f3) += deg v D(f1,f4)
-// gives J = (Jacc + Jacc^T)/4 and K = (Kacc + Kacc^T)/8.  Each target is a
-// dot product over the quartet's block computed by one lane, then one
-// atomic add per target element into the n x n accumulator (L2 resident).
-#include "eri.cuh"
+// eri.cu -- constant tables of the shell-quartet kernels and the class
+// dispatcher.  The kernel template is in eri_kernel.cuh; every kernel of
+// eri_kernels.inc is instantiated in its own translation unit (generated by
+// the Makefile), so the 110 instantiations compile in parallel.
+#include "eri_kernel.cuh"
+#include "eri_reg.cuh"
+#include "eri_smem.cuh"
 
 namespace pg {
 
@@ -51,338 +28,71 @@ cudaError_t upload_rys_constants(const RysConst &rc)
     return e;
 }
 
-constexpr double kSR = 34.98683665524972497;   // 2 pi^(5/2)
-constexpr int kRysDeg = 11;
+#define PG_KERNEL(la, lb, lc, ld, sw)                                                              \
+    extern template cudaError_t launch_one<la, lb, lc, ld, 1>(const EriArgs &, cudaStream_t, int); \
+    extern template cudaError_t launch_one<la, lb, lc, ld, 2>(const EriArgs &, cudaStream_t, int);
+#include "eri_kernels.inc"
+#undef PG_KERNEL
 
-constexpr int binom(int n, int k)
-{
-    int r = 1;
-    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
-    return r;
-}
-
-constexpr int pick_tq(int ncart_total)
-{
-    return ncart_total <= 12 ? 1
-         : ncart_total <= 40 ? 2
-         : ncart_total <= 120 ? 4
-         : ncart_total <= 300 ? 8
-         : ncart_total <= 700 ? 16
-         : ncart_total <= 1500 ? 32
-         : ncart_total <= 3000 ? 64 : 128;
-}
-
-template <int LA, int LB, int LC, int LD>
-struct ClassShape {
-    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    static constexpr int NCART = NA * NB * NC * ND;
-    static constexpr int L12 = LA + LB, L34 = LC + LD;
-    static constexpr int NR = (L12 + L34) / 2 + 1;
-    static constexpr int TSZ = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
-    static constexpr int TQ = pick_tq(NCART);
-    static constexpr int BLK = 128;
-    static constexpr int NTEAM = BLK / TQ;
-    static constexpr int SM_TEAM = 2 * NR + 3 * NR * TSZ + NCART;   // doubles
-    static constexpr size_t SMEM = sizeof(double) * SM_TEAM * NTEAM;
-};
-
-// 2-D recursion (rys.c:2269-2293 in the reference) and binomial transfer
-// (rys.c:2295-2336) for one root and one Cartesian direction; writes
-// I[a][b][c][d] into tab[idx * NR] with idx = ((a(LB+1)+b)(LC+1)+c)(LD+1)+d.
-template <int LA, int LB, int LC, int LD, int NR>
-__device__ __forceinline__ void vrr_hrr(double *__restrict__ tab, double g00, double B00, double B10,
-                                        double B01, double C, double Cp, double ab, double cd)
-{
-    constexpr int L12 = LA + LB, L34 = LC + LD;
-    double G[L12 + 1][L34 + 1];
-    G[0][0] = g00;
-    if (L12 > 0) G[1][0] = C * g00;
-#pragma unroll
-    for (int i = 1; i < L12; ++i) G[i + 1][0] = i * B10 * G[i - 1][0] + C * G[i][0];
-#pragma unroll
-    for (int j = 0; j < L34; ++j) {
-#pragma unroll
-        for (int i = 0; i <= L12; ++i) {
-            double v = Cp * G[i][j];
-            if (j > 0) v = fma(j * B01, G[i][j - 1], v);
-            if (i > 0) v = fma(i * B00, G[i - 1][j], v);
-            G[i][j + 1] = v;
-        }
+// Quartet class (LA LB | LC LD) of a list whose entries are (bra, ket) pairs;
+// classes listed with swap = 1 run on the kernel of (LC LD | LA LB).
+#define PG_KERNEL(la, lb, lc, ld, sw)                                                        \
+    if ((sw == 0 && LA == la && LB == lb && LC == lc && LD == ld) ||                        \
+        (sw == 1 && LA == lc && LB == ld && LC == la && LD == lb)) {                        \
+        EriArgs b = a;                                                                       \
+        b.swap = sw;                                                                         \
+        return a.mode == MODE_UHF ? launch_one<la, lb, lc, ld, 2>(b, stream, num_sms)       \
+                                  : launch_one<la, lb, lc, ld, 1>(b, stream, num_sms);      \
     }
-    // ket transfer H[i][c][d] = sum_k C(d,k) cd^k G[i][c+d-k], then bra
-    double cdp[LD + 1], abp[LB + 1];
-    cdp[0] = 1.0;
-#pragma unroll
-    for (int k = 1; k <= LD; ++k) cdp[k] = cdp[k - 1] * cd;
-    abp[0] = 1.0;
-#pragma unroll
-    for (int k = 1; k <= LB; ++k) abp[k] = abp[k - 1] * ab;
-#pragma unroll
-    for (int a = 0; a <= LA; ++a)
-#pragma unroll
-        for (int b = 0; b <= LB; ++b)
-#pragma unroll
-            for (int c = 0; c <= LC; ++c)
-#pragma unroll
-                for (int d = 0; d <= LD; ++d) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int i = 0; i <= b; ++i) {
-                        double t = 0.0;
-#pragma unroll
-                        for (int k = 0; k <= d; ++k) t = fma(binom(d, k) * cdp[k], G[a + b - i][c + d - k], t);
-                        s = fma(binom(b, i) * abp[i], t, s);
-                    }
-                    const int idx = ((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d;
-                    tab[idx * NR] = s;
-                }
-}
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) eri_class_kernel(const EriArgs args)
+#define PG_REG(la, lb, lc, ld)                                                                    \
+    extern template cudaError_t launch_reg<la, lb, lc, ld, 1>(const EriArgs &, cudaStream_t, int); \
+    extern template cudaError_t launch_reg<la, lb, lc, ld, 2>(const EriArgs &, cudaStream_t, int);
+#include "eri_reg_classes.inc"
+#undef PG_REG
+
+#define PG_CLASS(la, lb, lc, ld) \
+    extern template cudaError_t launch_smem<la, lb, lc, ld>(const EriArgs &, cudaStream_t, int);
+#include "eri_classes.inc"
+#undef PG_CLASS
+
+bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 {
-    using S = ClassShape<LA, LB, LC, LD>;
-    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCART = S::NCART;
-    constexpr int NR = S::NR, TSZ = S::TSZ, TQ = S::TQ, NTEAM = S::NTEAM;
-    extern __shared__ double smem[];
-    __shared__ int s_np[NTEAM];
-    __shared__ int s_maxp;
-
-    const int team = threadIdx.x / TQ, lane = threadIdx.x % TQ;
-    double *s_rw = smem + team * S::SM_TEAM;   // nodes [0, NR), weights [NR, 2NR)
-    double *s_tab = s_rw + 2 * NR;             // [3][TSZ][NR]
-    double *s_out = s_tab + 3 * NR * TSZ;      // [NCART]
-
-    for (long long base = (long long)blockIdx.x * NTEAM; base < args.nquart;
-         base += (long long)gridDim.x * NTEAM) {
-        const long long qi = base + team;
-        const bool active = qi < args.nquart;
-        int u = 0, v = 0, npb = 0, npk = 0, pb0 = 0, pk0 = 0;
-        double ax = 0, ay = 0, az = 0, abx = 0, aby = 0, abz = 0;
-        double cx = 0, cy = 0, cz = 0, cdx = 0, cdy = 0, cdz = 0;
-        if (active) {
-            int2 q = args.quart[qi];
-            u = q.x;
-            v = q.y;
-            npb = args.pr.pnum[u];
-            npk = args.pr.pnum[v];
-            pb0 = args.pr.pstart[u];
-            pk0 = args.pr.pstart[v];
-            ax = args.pr.ax[u]; ay = args.pr.ay[u]; az = args.pr.az[u];
-            abx = args.pr.abx[u]; aby = args.pr.aby[u]; abz = args.pr.abz[u];
-            cx = args.pr.ax[v]; cy = args.pr.ay[v]; cz = args.pr.az[v];
-            cdx = args.pr.abx[v]; cdy = args.pr.aby[v]; cdz = args.pr.abz[v];
-        }
-        for (int c = lane; c < NCART; c += TQ) s_out[c] = 0.0;
-        if (lane == 0) s_np[team] = npb * npk;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int m = 0;
-            for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
-            s_maxp = m;
-        }
-        __syncthreads();
-        const int maxp = s_maxp;
-
-        for (int ip = 0; ip < maxp; ++ip) {
-            bool work = active && ip < npb * npk;
-            double p = 1, q = 1, sr = 0, pax = 0, pay = 0, paz = 0, qcx = 0, qcy = 0, qcz = 0;
-            double pqx = 0, pqy = 0, pqz = 0;
-            if (work) {
-                const int ib = pb0 + ip / npk, ik = pk0 + ip % npk;
-                p = args.pp.p[ib];
-                q = args.pp.p[ik];
-                const double Px = args.pp.px[ib], Py = args.pp.py[ib], Pz = args.pp.pz[ib];
-                const double Qx = args.pp.px[ik], Qy = args.pp.py[ik], Qz = args.pp.pz[ik];
-                const double ppq = p + q, rs = rsqrt(ppq);
-                const double pre = kSR * args.pp.cut[ib] * args.pp.cut[ik] * rs;
-                if (pre < args.prim_cut) {    // primitive cut of twoints.c:109-111
-                    work = false;
-                } else {
-                    sr = kSR * args.pp.K[ib] * args.pp.K[ik] * rs;
-                    pax = Px - ax; pay = Py - ay; paz = Pz - az;
-                    qcx = Qx - cx; qcy = Qy - cy; qcz = Qz - cz;
-                    pqx = Px - Qx; pqy = Py - Qy; pqz = Pz - Qz;
-                    const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
-                    for (int f = lane; f < 2 * NR; f += TQ)
-                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg);
-                }
-            }
-            __syncthreads();
-            if (work) {
-                const double ppq = p + q;
-                for (int j = lane; j < 3 * NR; j += TQ) {
-                    const int r = j / 3, dim = j - 3 * r;
-                    const double x = s_rw[r], w = s_rw[NR + r];
-                    const double f = x / ppq, B00 = 0.5 * f;
-                    const double B10 = (0.5 - B00 * q) / p, B01 = (0.5 - B00 * p) / q;
-                    const double pa = dim == 0 ? pax : (dim == 1 ? pay : paz);
-                    const double qc = dim == 0 ? qcx : (dim == 1 ? qcy : qcz);
-                    const double pq = dim == 0 ? pqx : (dim == 1 ? pqy : pqz);
-                    const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
-                    const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                    vrr_hrr<LA, LB, LC, LD, NR>(s_tab + dim * TSZ * NR + r, dim == 2 ? w * sr : 1.0, B00, B10,
-                                                B01, pa - q * pq * f, qc + p * pq * f, ab, cd);
-                }
-            }
-            __syncthreads();
-            if (work) {
-                for (int c = lane; c < NCART; c += TQ) {
-                    const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
-                    const int ea = c_cart[LA][ia], eb = c_cart[LB][ib], ec = c_cart[LC][ic], ed = c_cart[LD][id];
-                    const int ix = ((((ea & 15) * (LB + 1) + (eb & 15)) * (LC + 1) + (ec & 15)) * (LD + 1) + (ed & 15));
-                    const int iy = (((((ea >> 4) & 15) * (LB + 1) + ((eb >> 4) & 15)) * (LC + 1) + ((ec >> 4) & 15)) *
-                                        (LD + 1) + ((ed >> 4) & 15));
-                    const int iz = ((((ea >> 8) * (LB + 1) + (eb >> 8)) * (LC + 1) + (ec >> 8)) * (LD + 1) + (ed >> 8));
-                    const double *tx = s_tab + ix * NR, *ty = s_tab + (TSZ + iy) * NR, *tz = s_tab + (2 * TSZ + iz) * NR;
-                    double s = 0.0;
-#pragma unroll
-                    for (int r = 0; r < NR; ++r) s = fma(tx[r] * ty[r], tz[r], s);
-                    s_out[c] += s;
-                }
-            }
-            __syncthreads();
-        }
-
-        // ------------------------------------------------ digestion / export
-        if (active) {
-            // component factors (basis.c:309-319)
-            for (int c = lane; c < NCART; c += TQ) {
-                const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
-                s_out[c] *= c_norm[LA][ia] * c_norm[LB][ib] * c_norm[LC][ic] * c_norm[LD][id];
-            }
-        }
-        __syncthreads();
-        if (active) {
-            if (args.mode == MODE_EXPORT) {
-                double *o = args.out + args.out_off[qi];
-                for (int c = lane; c < NCART; c += TQ) o[c] = s_out[c];
-            } else {
-                const int n = args.n;
-                const int fa = args.pr.fa[u], fb = args.pr.fb[u], fc = args.pr.fa[v], fd = args.pr.fb[v];
-                const bool sab = args.pr.sa[u] == args.pr.sb[u], scd = args.pr.sa[v] == args.pr.sb[v];
-                const double deg = (sab ? 1.0 : 2.0) * (scd ? 1.0 : 2.0) * (u == v ? 1.0 : 2.0);
-                const int mode = args.mode;
-                const double sJ = mode == MODE_RHF ? 0.5 * deg : 0.25 * deg;
-                const double sK = 0.125 * deg;
-                const double *D0 = args.D0, *D1 = args.D1;
-                constexpr int T0 = NA * NB, T1 = T0 + NC * ND, T2 = T1 + NA * NC, T3 = T2 + NA * ND,
-                              T4 = T3 + NB * NC, T5 = T4 + NB * ND;
-                for (int t = lane; t < T5; t += TQ) {
-                    if (t < T1) {
-                        // Coulomb: J(ab) over kets or J(cd) over bras, density Dsum
-                        double s = 0.0;
-                        int row, col;
-                        if (t < T0) {
-                            const int i = t / NB, j = t % NB;
-                            row = fa + i; col = fb + j;
-                            for (int k = 0; k < NC; ++k)
-                                for (int l = 0; l < ND; ++l) {
-                                    double d = __ldg(D0 + (size_t)(fc + k) * n + fd + l);
-                                    if (mode == MODE_UHF) d += __ldg(D1 + (size_t)(fc + k) * n + fd + l);
-                                    s = fma(s_out[((i * NB + j) * NC + k) * ND + l], d, s);
-                                }
-                        } else {
-                            const int tt = t - T0, k = tt / ND, l = tt % ND;
-                            row = fc + k; col = fd + l;
-                            for (int i = 0; i < NA; ++i)
-                                for (int j = 0; j < NB; ++j) {
-                                    double d = __ldg(D0 + (size_t)(fa + i) * n + fb + j);
-                                    if (mode == MODE_UHF) d += __ldg(D1 + (size_t)(fa + i) * n + fb + j);
-                                    s = fma(s_out[((i * NB + j) * NC + k) * ND + l], d, s);
-                                }
-                        }
-                        s *= sJ;
-                        atomicAdd(args.A0 + (size_t)row * n + col, s);
-                        if (mode == MODE_UHF) atomicAdd(args.A1 + (size_t)row * n + col, s);
-                    } else {
-                        // exchange: four index pairings
-                        double s0 = 0.0, s1 = 0.0;
-                        int row, col;
-                        const bool two = mode == MODE_UHF;
-                        if (t < T2) {          // K(a,c) over (b,d)
-                            const int tt = t - T1, i = tt / NC, k = tt % NC;
-                            row = fa + i; col = fc + k;
-                            for (int j = 0; j < NB; ++j)
-                                for (int l = 0; l < ND; ++l) {
-                                    const size_t di = (size_t)(fb + j) * n + fd + l;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
-                                    s0 = fma(vv, __ldg(D0 + di), s0);
-                                    if (two) s1 = fma(vv, __ldg(D1 + di), s1);
-                                }
-                        } else if (t < T3) {   // K(a,d) over (b,c)
-                            const int tt = t - T2, i = tt / ND, l = tt % ND;
-                            row = fa + i; col = fd + l;
-                            for (int j = 0; j < NB; ++j)
-                                for (int k = 0; k < NC; ++k) {
-                                    const size_t di = (size_t)(fb + j) * n + fc + k;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
-                                    s0 = fma(vv, __ldg(D0 + di), s0);
-                                    if (two) s1 = fma(vv, __ldg(D1 + di), s1);
-                                }
-                        } else if (t < T4) {   // K(b,c) over (a,d)
-                            const int tt = t - T3, j = tt / NC, k = tt % NC;
-                            row = fb + j; col = fc + k;
-                            for (int i = 0; i < NA; ++i)
-                                for (int l = 0; l < ND; ++l) {
-                                    const size_t di = (size_t)(fa + i) * n + fd + l;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
-                                    s0 = fma(vv, __ldg(D0 + di), s0);
-                                    if (two) s1 = fma(vv, __ldg(D1 + di), s1);
-                                }
-                        } else {               // K(b,d) over (a,c)
-                            const int tt = t - T4, j = tt / ND, l = tt % ND;
-                            row = fb + j; col = fd + l;
-                            for (int i = 0; i < NA; ++i)
-                                for (int k = 0; k < NC; ++k) {
-                                    const size_t di = (size_t)(fa + i) * n + fc + k;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
-                                    s0 = fma(vv, __ldg(D0 + di), s0);
-                                    if (two) s1 = fma(vv, __ldg(D1 + di), s1);
-                                }
-                        }
-                        const size_t o = (size_t)row * n + col;
-                        if (mode == MODE_JK) {
-                            atomicAdd(args.A1 + o, sK * s0);
-                        } else {
-                            atomicAdd(args.A0 + o, -sK * s0);
-                            if (two) atomicAdd(args.A1 + o, -sK * s1);
-                        }
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
+    if (variant == 0 || variant == 2) return true;
+#define PG_REG(la, lb, lc, ld) \
+    if (LA == la && LB == lb && LC == lc && LD == ld) return variant == 1;
+#include "eri_reg_classes.inc"
+#undef PG_REG
+    return false;
 }
-
-template <int LA, int LB, int LC, int LD>
-static cudaError_t launch_one(const EriArgs &a, cudaStream_t stream, int num_sms)
-{
-    using S = ClassShape<LA, LB, LC, LD>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(eri_class_kernel<LA, LB, LC, LD>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    long long blocks = (a.nquart + S::NTEAM - 1) / S::NTEAM;
-    long long cap = (long long)num_sms * 16;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) return cudaSuccess;
-    eri_class_kernel<LA, LB, LC, LD><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
-    return cudaGetLastError();
-}
-
-#define PG_CLASS(la, lb, lc, ld)                                   \
-    if (LA == la && LB == lb && LC == lc && LD == ld)             \
-        return launch_one<la, lb, lc, ld>(a, stream, num_sms);
 
 cudaError_t launch_eri_class(int LA, int LB, int LC, int LD, const EriArgs &a, cudaStream_t stream,
-                             int num_sms)
+                             int num_sms, int variant)
 {
+    if (variant == 2) {
+#define PG_CLASS(la, lb, lc, ld)                                   \
+    if (LA == la && LB == lb && LC == lc && LD == ld) {           \
+        EriArgs b = a;                                              \
+        b.swap = 0;                                                 \
+        return launch_smem<la, lb, lc, ld>(b, stream, num_sms);    \
+    }
 #include "eri_classes.inc"
+#undef PG_CLASS
+        return cudaErrorInvalidValue;
+    }
+    if (variant == 1) {
+#define PG_REG(la, lb, lc, ld)                                                            \
+    if (LA == la && LB == lb && LC == lc && LD == ld) {                                  \
+        EriArgs b = a;                                                                     \
+        b.swap = 0;                                                                        \
+        return a.mode == MODE_UHF ? launch_reg<la, lb, lc, ld, 2>(b, stream, num_sms)     \
+                                  : launch_reg<la, lb, lc, ld, 1>(b, stream, num_sms);    \
+    }
+#include "eri_reg_classes.inc"
+#undef PG_REG
+        return cudaErrorInvalidValue;
+    }
+#include "eri_kernels.inc"
     return cudaErrorInvalidValue;
 }
 

@@ -34,6 +34,7 @@ struct EriArgs {
     const int2 *quart;      // (bra pair, ket pair), bra class >= ket class
     long long nquart;
     int mode;
+    int swap;               // 1: quart[] holds (ket pair, bra pair) of this kernel's class
     int n;                  // basis functions
     const double *D0, *D1;  // full n x n densities
     double *A0, *A1;        // n x n accumulators
@@ -47,8 +48,13 @@ struct EriArgs {
 
 // Launch the kernel of class (la lb | lc ld) on `stream`.  Returns a CUDA
 // error code (cudaSuccess on success).
+// variant 0: the lane-per-ket-component team kernel (eri_kernel.cuh, every
+// class); 1: the register-only kernel (eri_reg.cuh, the classes of
+// eri_reg_classes.inc); 2: the shared-memory team kernel (eri_smem.cuh,
+// every class).
 cudaError_t launch_eri_class(int la, int lb, int lc, int ld, const EriArgs &a, cudaStream_t stream,
-                             int num_sms);
+                             int num_sms, int variant = 0);
+bool eri_has_variant(int la, int lb, int lc, int ld, int variant);
 
 cudaError_t upload_rys_constants(const RysConst &rc);
 

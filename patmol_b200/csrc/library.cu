@@ -107,6 +107,7 @@ static int init_tables()
 struct ClassWork {
     int la, lb, lc, ld;
     long long offset, count;
+    int variant = 0;     // kernel variant chosen for this class (see tune_variants)
 };
 
 static int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
@@ -359,6 +360,65 @@ static int build_quartets(patgpu_basis *h)
     return 0;
 }
 
+// Kernel-variant autotuner: every class has the lane team kernel (0) and the
+// shared-memory team kernel (2); the small classes also have the
+// register-only kernel (1).  Each variant is timed on the class's own
+// quartet list and the fastest kept.  Runs once per quartet list, on a zero
+// density and the handle's own accumulator (the results are discarded).
+// PATGPU_VARIANT=lane|reg|smem forces a choice where it exists.
+static int ensure_work(patgpu_basis *h, bool two);
+
+static int tune_variants(patgpu_basis *h)
+{
+    const char *force = getenv("PATGPU_VARIANT");
+    int forced = -1;
+    if (force && !strcmp(force, "lane")) forced = 0;
+    if (force && !strcmp(force, "reg")) forced = 1;
+    if (force && !strcmp(force, "smem")) forced = 2;
+    for (auto &w : h->work) w.variant = 0;
+    if (h->work.empty()) return 0;
+    if (forced >= 0) {
+        for (auto &w : h->work)
+            if (eri_has_variant(w.la, w.lb, w.lc, w.ld, forced)) w.variant = forced;
+        return 0;
+    }
+    int rc = ensure_work(h, false);
+    if (rc) return rc;
+    const size_t nn = (size_t)h->n * h->n;
+    cudaStream_t s = h->stream;
+    PG_CUDA(cudaMemsetAsync(h->d_D0.p, 0, sizeof(double) * nn, s));
+    EriArgs a = h->base_args();
+    a.mode = MODE_RHF;
+    a.D0 = h->d_D0.as<double>();
+    a.A0 = h->d_A0.as<double>();
+    cudaEvent_t e0, e1;
+    PG_CUDA(cudaEventCreate(&e0));
+    PG_CUDA(cudaEventCreate(&e1));
+    for (auto &w : h->work) {
+        a.quart = h->d_quart.as<int2>() + w.offset;
+        a.nquart = w.count;
+        float best = 1e30f;
+        for (int var = 0; var <= 2; ++var) {
+            if (!eri_has_variant(w.la, w.lb, w.lc, w.ld, var)) continue;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {   // first launch warms up
+                PG_CUDA(cudaEventRecord(e0, s));
+                PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, var));
+                PG_CUDA(cudaEventRecord(e1, s));
+                PG_CUDA(cudaEventSynchronize(e1));
+                PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            }
+            if (ms < best) {
+                best = ms;
+                w.variant = var;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
 // ------------------------------------------------------- small kernels
 __global__ void unpack_kernel(const double *__restrict__ pk, double *__restrict__ full, int n)
 {
@@ -419,7 +479,7 @@ static int launch_fock(patgpu_basis *h, int mode, cudaStream_t s)
     for (auto &w : h->work) {
         a.quart = h->d_quart.as<int2>() + w.offset;
         a.nquart = w.count;
-        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms));
+        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant));
         ++launches;
     }
     PG_CUDA(cudaEventRecord(h->ev1, s));
@@ -564,6 +624,7 @@ int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off
     rc = build_pairs(h);
     if (!rc) rc = build_schwarz(h);
     if (!rc) rc = build_quartets(h);
+    if (!rc) rc = tune_variants(h);
     if (rc) {
         patgpu_basis_destroy(h);
         return rc;
@@ -589,7 +650,8 @@ int patgpu_set_quartets(patgpu_handle h, int start_shell, int rank, int nranks)
     h->start_shell = start_shell;
     h->rank = rank;
     h->nranks = nranks;
-    return build_quartets(h);
+    int rc = build_quartets(h);
+    return rc ? rc : tune_variants(h);
 }
 
 int patgpu_rhf_gmatrix(patgpu_handle h, const double *P, double *G)
@@ -628,7 +690,7 @@ int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, 
     for (auto &w : h->work) {
         a.quart = h->d_quart.as<int2>() + w.offset;
         a.nquart = w.count;
-        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms));
+        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant));
         ++launches;
     }
     PG_CUDA(cudaEventRecord(h->ev1, s));
@@ -721,7 +783,7 @@ int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double 
     for (auto &w : h->work) {
         a.quart = h->d_quart.as<int2>() + w.offset;
         a.nquart = w.count;
-        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms));
+        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant));
     }
     const long long no2 = (long long)n * (n + 1) / 2;
     finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(A, dG, n);

@@ -29,7 +29,8 @@ class PatgpuError(RuntimeError):
 def build(force: bool = False) -> str:
     """Compile libpatgpu.so for sm_100a (nvcc; no GPU needed)."""
     if force or not os.path.exists(LIB_PATH):
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc")], check=True)
+        subprocess.run(["make", "-s", f"-j{max(1, os.cpu_count() or 1)}", "-C", os.path.join(HERE, "csrc")],
+                       check=True)
     return LIB_PATH
 
 
