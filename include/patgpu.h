@@ -151,6 +151,17 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
                    const double *charge, const double *xyz, int skipcen, double *S, double *T,
                    double *H, double *Hdpm);
 
+/* Mixed precision (no counterpart in the reference, which is FP64
+ * throughout): quartets whose Schwarz bound Q_ab Q_cd lies between the
+ * screening threshold and tau_fp32 are computed with FP32 recursion,
+ * transfer and assembly, while roots, weights, prefactors and every J/K
+ * product and sum stay FP64; their integrals are below tau_fp32 in size, so
+ * the absolute error per integral is about 1e-7 tau_fp32.  0 turns it off
+ * (the default).  patgpu_mixed_stats returns how many quartets of this
+ * handle run in FP32. */
+int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32);
+int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32);
+
 /* Sizes of the handle: [0] basis functions, [1] shell pairs, [2] quartets
  * owned, [3] classes with work, [4] quartets before screening. */
 int patgpu_stats(patgpu_handle h, long long *out5);

@@ -51,14 +51,15 @@ cudaError_t upload_rys_constants(const RysConst &rc)
 #include "eri_reg_classes.inc"
 #undef PG_REG
 
-#define PG_CLASS(la, lb, lc, ld) \
-    extern template cudaError_t launch_smem<la, lb, lc, ld>(const EriArgs &, cudaStream_t, int);
+#define PG_CLASS(la, lb, lc, ld)                                                                       \
+    extern template cudaError_t launch_smem<la, lb, lc, ld, double>(const EriArgs &, cudaStream_t, int); \
+    extern template cudaError_t launch_smem<la, lb, lc, ld, float>(const EriArgs &, cudaStream_t, int);
 #include "eri_classes.inc"
 #undef PG_CLASS
 
 bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 {
-    if (variant == 0 || variant == 2) return true;
+    if (variant == 0 || variant == 2 || variant == 3) return true;
 #define PG_REG(la, lb, lc, ld) \
     if (LA == la && LB == lb && LC == lc && LD == ld) return variant == 1;
 #include "eri_reg_classes.inc"
@@ -69,12 +70,13 @@ bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 cudaError_t launch_eri_class(int LA, int LB, int LC, int LD, const EriArgs &a, cudaStream_t stream,
                              int num_sms, int variant)
 {
-    if (variant == 2) {
-#define PG_CLASS(la, lb, lc, ld)                                   \
-    if (LA == la && LB == lb && LC == lc && LD == ld) {           \
-        EriArgs b = a;                                              \
-        b.swap = 0;                                                 \
-        return launch_smem<la, lb, lc, ld>(b, stream, num_sms);    \
+    if (variant == 2 || variant == 3) {
+#define PG_CLASS(la, lb, lc, ld)                                                     \
+    if (LA == la && LB == lb && LC == lc && LD == ld) {                             \
+        EriArgs b = a;                                                                \
+        b.swap = 0;                                                                   \
+        return variant == 2 ? launch_smem<la, lb, lc, ld, double>(b, stream, num_sms) \
+                            : launch_smem<la, lb, lc, ld, float>(b, stream, num_sms); \
     }
 #include "eri_classes.inc"
 #undef PG_CLASS

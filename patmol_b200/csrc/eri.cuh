@@ -31,8 +31,17 @@ struct PrimDev {
 struct EriArgs {
     PairDev pr;
     PrimDev pp;
-    const int2 *quart;      // (bra pair, ket pair), bra class >= ket class
-    long long nquart;
+    const int2 *quart;      // list mode: (bra pair, ket pair), bra class >= ket class
+    long long nquart;       // work items of this launch
+    // implicit mode (no list): item qi is quartet k = qi*nranks + rank of the
+    // class's bra x ket pair space -- pairs u0+i, v0+j with (i, j) = (k / nv,
+    // k % nv), or the triangle j <= i when bra and ket are the same class --
+    // kept when tau_lo <= Q_u Q_v < tau_hi and its largest shell index is at
+    // least start_shell.
+    int implicit;
+    int u0, nu, v0, nv, same, rank, nranks, start_shell;
+    const double *Q;
+    double tau_lo, tau_hi;
     int mode;
     int swap;               // 1: quart[] holds (ket pair, bra pair) of this kernel's class
     int n;                  // basis functions
@@ -57,5 +66,43 @@ cudaError_t launch_eri_class(int la, int lb, int lc, int ld, const EriArgs &a, c
 bool eri_has_variant(int la, int lb, int lc, int ld, int variant);
 
 cudaError_t upload_rys_constants(const RysConst &rc);
+
+#ifdef __CUDACC__
+// Work item qi -> (bra pair u, ket pair v) in this kernel's orientation;
+// false when the item is screened out.
+__device__ __forceinline__ bool eri_quartet_at(const EriArgs &a, long long qi, int &u, int &v)
+{
+    int ub, vk;
+    if (!a.implicit) {
+        const int2 q = a.quart[qi];
+        ub = q.x;
+        vk = q.y;
+    } else {
+        const long long k = qi * a.nranks + a.rank;
+        long long i, j;
+        if (a.same) {
+            i = (long long)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
+            while (i * (i + 1) / 2 > k) --i;
+            while ((i + 1) * (i + 2) / 2 <= k) ++i;
+            j = k - i * (i + 1) / 2;
+            if (i >= a.nu) return false;
+        } else {
+            i = k / a.nv;
+            j = k - i * a.nv;
+            if (i >= a.nu) return false;
+        }
+        ub = a.u0 + (int)i;
+        vk = a.v0 + (int)j;
+        const double b = __ldg(a.Q + ub) * __ldg(a.Q + vk);
+        if (!(b >= a.tau_lo && b < a.tau_hi)) return false;
+        if (a.start_shell > 0 &&
+            max(max(a.pr.sa[ub], a.pr.sb[ub]), max(a.pr.sa[vk], a.pr.sb[vk])) < a.start_shell)
+            return false;
+    }
+    u = a.swap ? vk : ub;
+    v = a.swap ? ub : vk;
+    return true;
+}
+#endif
 
 }  // namespace pg

@@ -95,6 +95,10 @@ struct Shape {
     static constexpr int NTEAM = NT1 > 0 ? NT1 : 1;
     static constexpr int BLK = ((NTEAM * TQ + 31) / 32) * 32;
     static constexpr size_t SMEM = sizeof(double) * (size_t)SM_TEAM * NTEAM;
+    // resident blocks requested from the register allocator: at most 128
+    // registers a thread, so latency is hidden by occupancy (measured: 96
+    // spills too much, 255 leaves 8 warps an SM)
+    static constexpr int MINB = (65536 / (BLK * 128)) > 0 ? 65536 / (BLK * 128) : 1;
 };
 
 // 2-D recursion and binomial transfer for one root and one direction;
@@ -175,7 +179,8 @@ __device__ __forceinline__ void assemble(double (&acc)[CHN], const double *__res
 }
 
 template <int LA, int LB, int LC, int LD, int NDEN>
-__global__ void __launch_bounds__(Shape<LA, LB, LC, LD, NDEN>::BLK) eri_class_kernel(const EriArgs args)
+__global__ void __launch_bounds__(Shape<LA, LB, LC, LD, NDEN>::BLK, Shape<LA, LB, LC, LD, NDEN>::MINB)
+eri_class_kernel(const EriArgs args)
 {
     using S = Shape<LA, LB, LC, LD, NDEN>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NAB = S::NAB, NCD = S::NCD;
@@ -206,15 +211,12 @@ __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, NDEN>::BLK) eri_class_ke
     for (long long base = (long long)blockIdx.x * NTEAM; base < args.nquart;
          base += (long long)gridDim.x * NTEAM) {
         const long long qi = base + team;
-        const bool active = in_team && qi < args.nquart;
         int u = 0, v = 0, npb = 0, npk = 0, pb0 = 0, pk0 = 0;
+        const bool active = in_team && qi < args.nquart && eri_quartet_at(args, qi, u, v);
         double ax = 0, ay = 0, az = 0, abx = 0, aby = 0, abz = 0;
         double cx = 0, cy = 0, cz = 0, cdx = 0, cdy = 0, cdz = 0;
         int fa = 0, fb = 0, fc = 0, fd = 0;
         if (active) {
-            const int2 q = args.quart[qi];
-            u = args.swap ? q.y : q.x;
-            v = args.swap ? q.x : q.y;
             npb = args.pr.pnum[u];
             npk = args.pr.pnum[v];
             pb0 = args.pr.pstart[u];

@@ -72,7 +72,7 @@ __device__ __forceinline__ void vrr_hrr_reg(double (&t)[RegShape<LA, LB, LC, LD>
 }
 
 template <int LA, int LB, int LC, int LD, int NDEN>
-__global__ void __launch_bounds__(128) eri_reg_kernel(const EriArgs args)
+__global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 {
     using S = RegShape<LA, LB, LC, LD>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NAB = S::NAB, NCD = S::NCD;
@@ -84,8 +84,8 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const EriArgs args)
 
     for (long long qi = (long long)blockIdx.x * blockDim.x + threadIdx.x; qi < args.nquart;
          qi += (long long)gridDim.x * blockDim.x) {
-        const int2 q = args.quart[qi];
-        const int u = args.swap ? q.y : q.x, v = args.swap ? q.x : q.y;
+        int u, v;
+        if (!eri_quartet_at(args, qi, u, v)) continue;
         const int npb = args.pr.pnum[u], npk = args.pr.pnum[v];
         const int pb0 = args.pr.pstart[u], pk0 = args.pr.pstart[v];
         const double ax = args.pr.ax[u], ay = args.pr.ay[u], az = args.pr.az[u];
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const EriArgs args)
                 const double qcx = Qx - cx, qcy = Qy - cy, qcz = Qz - cz;
                 const double pqx = Px - Qx, pqy = Py - Qy, pqz = Pz - Qz;
                 const double T = p * qx / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
-#pragma unroll
+#pragma unroll 1
                 for (int r = 0; r < NR; ++r) {
                     const double x = rys_eval(NR, r, T, c_rys, args.rys_coef, kRysDeg);
                     const double w = rys_eval(NR, NR + r, T, c_rys, args.rys_coef, kRysDeg);

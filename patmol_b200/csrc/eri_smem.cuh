@@ -4,6 +4,11 @@
 // J/K target is a dot product over the block computed by one lane.  Same
 // mathematics and digestion rule as eri_kernel.cuh (which see); the
 // autotuner picks, per class, whichever variant runs fastest.
+//
+// The arithmetic type R of the recursion, tables and integrals is a template
+// parameter: R = float gives the mixed-precision path for quartets whose
+// Schwarz bound is small -- roots and weights, prefactors and T are still
+// FP64, and every digestion product and J/K sum is formed in FP64.
 #pragma once
 #include "eri_kernel.cuh"
 
@@ -21,7 +26,7 @@ constexpr int pick_tq(int ncart_total)
          : ncart_total <= 3000 ? 64 : 128;
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 struct SmemShape {
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     static constexpr int NCART = NA * NB * NC * ND;
@@ -31,19 +36,20 @@ struct SmemShape {
     static constexpr int TQ = pick_tq(NCART);
     static constexpr int BLK = 128;
     static constexpr int NTEAM = BLK / TQ;
-    static constexpr int SM_TEAM = 2 * NR + 3 * NR * TSZ + NCART;   // doubles
-    static constexpr size_t SMEM = sizeof(double) * SM_TEAM * NTEAM;
+    // bytes per team: roots and weights (FP64), tables and integrals (R)
+    static constexpr int TEAM_BYTES = ((16 * NR + (int)sizeof(R) * (3 * NR * TSZ + NCART)) + 15) / 16 * 16;
+    static constexpr size_t SMEM = (size_t)TEAM_BYTES * NTEAM;
 };
 
 // 2-D recursion (rys.c:2269-2293 in the reference) and binomial transfer
 // (rys.c:2295-2336) for one root and one Cartesian direction; writes
 // I[a][b][c][d] into tab[idx * NR] with idx = ((a(LB+1)+b)(LC+1)+c)(LD+1)+d.
-template <int LA, int LB, int LC, int LD, int NR>
-__device__ __forceinline__ void vrr_hrr_smem(double *__restrict__ tab, double g00, double B00, double B10,
-                                        double B01, double C, double Cp, double ab, double cd)
+template <int LA, int LB, int LC, int LD, int NR, typename R>
+__device__ __forceinline__ void vrr_hrr_smem(R *__restrict__ tab, R g00, R B00, R B10, R B01, R C, R Cp, R ab,
+                                             R cd)
 {
     constexpr int L12 = LA + LB, L34 = LC + LD;
-    double G[L12 + 1][L34 + 1];
+    R G[L12 + 1][L34 + 1];
     G[0][0] = g00;
     if (L12 > 0) G[1][0] = C * g00;
 #pragma unroll
@@ -52,18 +58,18 @@ __device__ __forceinline__ void vrr_hrr_smem(double *__restrict__ tab, double g0
     for (int j = 0; j < L34; ++j) {
 #pragma unroll
         for (int i = 0; i <= L12; ++i) {
-            double v = Cp * G[i][j];
-            if (j > 0) v = fma(j * B01, G[i][j - 1], v);
-            if (i > 0) v = fma(i * B00, G[i - 1][j], v);
+            R v = Cp * G[i][j];
+            if (j > 0) v = fma(R(j) * B01, G[i][j - 1], v);
+            if (i > 0) v = fma(R(i) * B00, G[i - 1][j], v);
             G[i][j + 1] = v;
         }
     }
     // ket transfer H[i][c][d] = sum_k C(d,k) cd^k G[i][c+d-k], then bra
-    double cdp[LD + 1], abp[LB + 1];
-    cdp[0] = 1.0;
+    R cdp[LD + 1], abp[LB + 1];
+    cdp[0] = R(1);
 #pragma unroll
     for (int k = 1; k <= LD; ++k) cdp[k] = cdp[k - 1] * cd;
-    abp[0] = 1.0;
+    abp[0] = R(1);
 #pragma unroll
     for (int k = 1; k <= LB; ++k) abp[k] = abp[k - 1] * ab;
 #pragma unroll
@@ -74,23 +80,23 @@ __device__ __forceinline__ void vrr_hrr_smem(double *__restrict__ tab, double g0
             for (int c = 0; c <= LC; ++c)
 #pragma unroll
                 for (int d = 0; d <= LD; ++d) {
-                    double s = 0.0;
+                    R s = R(0);
 #pragma unroll
                     for (int i = 0; i <= b; ++i) {
-                        double t = 0.0;
+                        R t = R(0);
 #pragma unroll
-                        for (int k = 0; k <= d; ++k) t = fma(binom(d, k) * cdp[k], G[a + b - i][c + d - k], t);
-                        s = fma(binom(b, i) * abp[i], t, s);
+                        for (int k = 0; k <= d; ++k) t = fma(R(binom(d, k)) * cdp[k], G[a + b - i][c + d - k], t);
+                        s = fma(R(binom(b, i)) * abp[i], t, s);
                     }
                     const int idx = ((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d;
                     tab[idx * NR] = s;
                 }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
 {
-    using S = SmemShape<LA, LB, LC, LD>;
+    using S = SmemShape<LA, LB, LC, LD, R>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCART = S::NCART;
     constexpr int NR = S::NR, TSZ = S::TSZ, TQ = S::TQ, NTEAM = S::NTEAM;
     extern __shared__ double smem[];
@@ -98,21 +104,18 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
     __shared__ int s_maxp;
 
     const int team = threadIdx.x / TQ, lane = threadIdx.x % TQ;
-    double *s_rw = smem + team * S::SM_TEAM;   // nodes [0, NR), weights [NR, 2NR)
-    double *s_tab = s_rw + 2 * NR;             // [3][TSZ][NR]
-    double *s_out = s_tab + 3 * NR * TSZ;      // [NCART]
+    double *s_rw = reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + team * S::TEAM_BYTES);  // nodes, weights
+    R *s_tab = reinterpret_cast<R *>(s_rw + 2 * NR);   // [3][TSZ][NR]
+    R *s_out = s_tab + 3 * NR * TSZ;                   // [NCART]
 
     for (long long base = (long long)blockIdx.x * NTEAM; base < args.nquart;
          base += (long long)gridDim.x * NTEAM) {
         const long long qi = base + team;
-        const bool active = qi < args.nquart;
         int u = 0, v = 0, npb = 0, npk = 0, pb0 = 0, pk0 = 0;
+        const bool active = qi < args.nquart && eri_quartet_at(args, qi, u, v);
         double ax = 0, ay = 0, az = 0, abx = 0, aby = 0, abz = 0;
         double cx = 0, cy = 0, cz = 0, cdx = 0, cdy = 0, cdz = 0;
         if (active) {
-            int2 q = args.quart[qi];
-            u = q.x;
-            v = q.y;
             npb = args.pr.pnum[u];
             npk = args.pr.pnum[v];
             pb0 = args.pr.pstart[u];
@@ -122,7 +125,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
             cx = args.pr.ax[v]; cy = args.pr.ay[v]; cz = args.pr.az[v];
             cdx = args.pr.abx[v]; cdy = args.pr.aby[v]; cdz = args.pr.abz[v];
         }
-        for (int c = lane; c < NCART; c += TQ) s_out[c] = 0.0;
+        for (int c = lane; c < NCART; c += TQ) s_out[c] = R(0);
         if (lane == 0) s_np[team] = npb * npk;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -170,8 +173,9 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                     const double pq = dim == 0 ? pqx : (dim == 1 ? pqy : pqz);
                     const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
                     const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                    vrr_hrr_smem<LA, LB, LC, LD, NR>(s_tab + dim * TSZ * NR + r, dim == 2 ? w * sr : 1.0, B00, B10,
-                                                B01, pa - q * pq * f, qc + p * pq * f, ab, cd);
+                    vrr_hrr_smem<LA, LB, LC, LD, NR, R>(s_tab + dim * TSZ * NR + r, R(dim == 2 ? w * sr : 1.0), R(B00),
+                                                        R(B10), R(B01), R(pa - q * pq * f), R(qc + p * pq * f), R(ab),
+                                                        R(cd));
                 }
             }
             __syncthreads();
@@ -183,8 +187,8 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                     const int iy = (((((ea >> 4) & 15) * (LB + 1) + ((eb >> 4) & 15)) * (LC + 1) + ((ec >> 4) & 15)) *
                                         (LD + 1) + ((ed >> 4) & 15));
                     const int iz = ((((ea >> 8) * (LB + 1) + (eb >> 8)) * (LC + 1) + (ec >> 8)) * (LD + 1) + (ed >> 8));
-                    const double *tx = s_tab + ix * NR, *ty = s_tab + (TSZ + iy) * NR, *tz = s_tab + (2 * TSZ + iz) * NR;
-                    double s = 0.0;
+                    const R *tx = s_tab + ix * NR, *ty = s_tab + (TSZ + iy) * NR, *tz = s_tab + (2 * TSZ + iz) * NR;
+                    R s = R(0);
 #pragma unroll
                     for (int r = 0; r < NR; ++r) s = fma(tx[r] * ty[r], tz[r], s);
                     s_out[c] += s;
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
             // component factors (basis.c:309-319)
             for (int c = lane; c < NCART; c += TQ) {
                 const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
-                s_out[c] *= c_norm[LA][ia] * c_norm[LB][ib] * c_norm[LC][ic] * c_norm[LD][id];
+                s_out[c] *= R(c_norm[LA][ia] * c_norm[LB][ib] * c_norm[LC][ic] * c_norm[LD][id]);
             }
         }
         __syncthreads();
@@ -229,7 +233,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                                 for (int l = 0; l < ND; ++l) {
                                     double d = __ldg(D0 + (size_t)(fc + k) * n + fd + l);
                                     if (mode == MODE_UHF) d += __ldg(D1 + (size_t)(fc + k) * n + fd + l);
-                                    s = fma(s_out[((i * NB + j) * NC + k) * ND + l], d, s);
+                                    s = fma((double)s_out[((i * NB + j) * NC + k) * ND + l], d, s);
                                 }
                         } else {
                             const int tt = t - T0, k = tt / ND, l = tt % ND;
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                                 for (int j = 0; j < NB; ++j) {
                                     double d = __ldg(D0 + (size_t)(fa + i) * n + fb + j);
                                     if (mode == MODE_UHF) d += __ldg(D1 + (size_t)(fa + i) * n + fb + j);
-                                    s = fma(s_out[((i * NB + j) * NC + k) * ND + l], d, s);
+                                    s = fma((double)s_out[((i * NB + j) * NC + k) * ND + l], d, s);
                                 }
                         }
                         s *= sJ;
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                             for (int j = 0; j < NB; ++j)
                                 for (int l = 0; l < ND; ++l) {
                                     const size_t di = (size_t)(fb + j) * n + fd + l;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
+                                    const double vv = (double)s_out[((i * NB + j) * NC + k) * ND + l];
                                     s0 = fma(vv, __ldg(D0 + di), s0);
                                     if (two) s1 = fma(vv, __ldg(D1 + di), s1);
                                 }
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                             for (int j = 0; j < NB; ++j)
                                 for (int k = 0; k < NC; ++k) {
                                     const size_t di = (size_t)(fb + j) * n + fc + k;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
+                                    const double vv = (double)s_out[((i * NB + j) * NC + k) * ND + l];
                                     s0 = fma(vv, __ldg(D0 + di), s0);
                                     if (two) s1 = fma(vv, __ldg(D1 + di), s1);
                                 }
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                             for (int i = 0; i < NA; ++i)
                                 for (int l = 0; l < ND; ++l) {
                                     const size_t di = (size_t)(fa + i) * n + fd + l;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
+                                    const double vv = (double)s_out[((i * NB + j) * NC + k) * ND + l];
                                     s0 = fma(vv, __ldg(D0 + di), s0);
                                     if (two) s1 = fma(vv, __ldg(D1 + di), s1);
                                 }
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
                             for (int i = 0; i < NA; ++i)
                                 for (int k = 0; k < NC; ++k) {
                                     const size_t di = (size_t)(fa + i) * n + fc + k;
-                                    const double vv = s_out[((i * NB + j) * NC + k) * ND + l];
+                                    const double vv = (double)s_out[((i * NB + j) * NC + k) * ND + l];
                                     s0 = fma(vv, __ldg(D0 + di), s0);
                                     if (two) s1 = fma(vv, __ldg(D1 + di), s1);
                                 }
@@ -305,13 +309,13 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 cudaError_t launch_smem(const EriArgs &a, cudaStream_t stream, int num_sms)
 {
-    using S = SmemShape<LA, LB, LC, LD>;
+    using S = SmemShape<LA, LB, LC, LD, R>;
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(eri_smem_kernel<LA, LB, LC, LD>,
+        cudaError_t e = cudaFuncSetAttribute(eri_smem_kernel<LA, LB, LC, LD, R>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
         configured = true;
@@ -320,7 +324,7 @@ cudaError_t launch_smem(const EriArgs &a, cudaStream_t stream, int num_sms)
     long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
-    eri_smem_kernel<LA, LB, LC, LD><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
+    eri_smem_kernel<LA, LB, LC, LD, R><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
     return cudaGetLastError();
 }
 

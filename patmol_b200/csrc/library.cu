@@ -106,8 +106,11 @@ static int init_tables()
 // ------------------------------------------------------------------ handle
 struct ClassWork {
     int la, lb, lc, ld;
-    long long offset, count;
-    int variant = 0;     // kernel variant chosen for this class (see tune_variants)
+    long long offset, count;     // count: quartets this rank owns after screening
+    int variant = 0;             // kernel variant chosen for this class (see tune_variants)
+    int u0 = 0, nu = 0, v0 = 0, nv = 0, same = 0;   // bra and ket pair ranges
+    long long total = 0;         // unscreened quartets of the class (all ranks)
+    long long items = 0;         // work items of this rank: ceil((total - rank) / nranks)
 };
 
 static int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
@@ -120,6 +123,8 @@ struct patgpu_basis {
     std::vector<int> l, cen, off, nst, poff;
     std::vector<double> al, co, q, xyz;
     double tau = 0.0;
+    double tau_mix = 0.0;            // > 0: quartets with bounds in [tau, tau_mix) run in FP32
+    long long nquart_fp32 = 0;
     int start_shell = 0, rank = 0, nranks = 1;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
@@ -130,10 +135,9 @@ struct patgpu_basis {
     std::vector<double> pp_p, pp_px, pp_py, pp_pz, pp_K, pp_cut;
     std::vector<int> class_begin;   // pairs of class c: [class_begin[c], class_begin[c+1])
     pg::DBuf d_psa, d_psb, d_pfa, d_pfb, d_pax, d_pay, d_paz, d_pabx, d_paby, d_pabz, d_pstart, d_pnum;
-    pg::DBuf d_pp_p, d_pp_px, d_pp_py, d_pp_pz, d_pp_K, d_pp_cut;
+    pg::DBuf d_pp_p, d_pp_px, d_pp_py, d_pp_pz, d_pp_K, d_pp_cut, d_Q;
     // quartets
     std::vector<pg::ClassWork> work;
-    pg::DBuf d_quart;
     long long nquart = 0, nquart_unscreened = 0;
     // work buffers
     pg::DBuf d_D0, d_D1, d_A0, d_A1, d_Pk0, d_Pk1, d_Gk0, d_Gk1, d_err;
@@ -324,11 +328,73 @@ static int build_schwarz(patgpu_basis *h)
     return 0;
 }
 
+// Arguments of the implicit (list-free) launch of class w: every work item
+// maps to one bra x ket pair combination, screened on the device.
+static EriArgs class_args(const patgpu_basis *h, const ClassWork &w, int mode, double tau_lo, double tau_hi)
+{
+    EriArgs a = h->base_args();
+    a.mode = mode;
+    a.implicit = 1;
+    a.u0 = w.u0;
+    a.nu = w.nu;
+    a.v0 = w.v0;
+    a.nv = w.nv;
+    a.same = w.same;
+    a.rank = h->rank;
+    a.nranks = h->nranks;
+    a.start_shell = h->start_shell;
+    a.Q = h->d_Q.as<double>();
+    a.tau_lo = tau_lo;
+    a.tau_hi = tau_hi;
+    a.nquart = w.items;
+    return a;
+}
+
+// Launch the class kernel(s) of w with the densities, accumulators and mode
+// carried by proto.
+// With mixed precision on, the class runs twice over its pair space: the
+// tuned FP64 kernel on the quartets whose bound is at least tau_mix, the FP32
+// kernel on those between the screening threshold and tau_mix.
+static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const EriArgs &proto, cudaStream_t s)
+{
+    const double lo = h->tau > 0.0 ? h->tau : -1.0;
+    const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
+    EriArgs a = class_args(h, w, proto.mode, mixed ? h->tau_mix : lo, INFINITY);
+    a.D0 = proto.D0;
+    a.D1 = proto.D1;
+    a.A0 = proto.A0;
+    a.A1 = proto.A1;
+    cudaError_t e = launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant);
+    if (e != cudaSuccess || !mixed) return e;
+    a.tau_lo = lo;
+    a.tau_hi = h->tau_mix;
+    return launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, 3);
+}
+
+__global__ void count_kernel(const EriArgs a, unsigned long long *cnt)
+{
+    unsigned long long c = 0;
+    for (long long qi = (long long)blockIdx.x * blockDim.x + threadIdx.x; qi < a.nquart;
+         qi += (long long)gridDim.x * blockDim.x) {
+        int u, v;
+        if (eri_quartet_at(a, qi, u, v)) ++c;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, c);
+}
+
+// Per class pair (bra class >= ket class): the pair ranges and the number of
+// quartets that survive screening on this rank (counted on the device, so no
+// quartet list is ever built; lists of 1e10 quartets would not fit).
 static int build_quartets(patgpu_basis *h)
 {
     h->work.clear();
-    std::vector<int2> all;
-    long long unscreened = 0;
+    long long unscreened = 0, owned = 0;
+    PG_CUDA(upload(h->d_Q, h->Q, h->stream));
+    DBuf dcnt;
+    PG_CUDA(dcnt.ensure(sizeof(unsigned long long) * 64));
+    PG_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long) * 64, h->stream));
+    std::vector<ClassWork> all;
     for (int cu = 0; cu < 10; ++cu)
         for (int cv = 0; cv <= cu; ++cv) {
             const int u0 = h->class_begin[cu], u1 = h->class_begin[cu + 1];
@@ -337,26 +403,31 @@ static int build_quartets(patgpu_basis *h)
             ClassWork w;
             class_ls(cu, w.la, w.lb);
             class_ls(cv, w.lc, w.ld);
+            w.u0 = u0; w.nu = u1 - u0; w.v0 = v0; w.nv = v1 - v0; w.same = cu == cv;
+            w.total = w.same ? (long long)w.nu * (w.nu + 1) / 2 : (long long)w.nu * w.nv;
+            w.items = w.total > h->rank ? (w.total - h->rank + h->nranks - 1) / h->nranks : 0;
             w.offset = (long long)all.size();
-            long long k = 0;
-            for (int u = u0; u < u1; ++u) {
-                const int vend = (cu == cv) ? u + 1 : v1;
-                const int mu = std::max(h->psa[u], h->psb[u]);
-                for (int v = v0; v < vend; ++v) {
-                    ++unscreened;
-                    if (h->tau > 0.0 && h->Q[u] * h->Q[v] < h->tau) continue;
-                    if (std::max(mu, std::max(h->psa[v], h->psb[v])) < h->start_shell) continue;
-                    if ((k++ % h->nranks) != h->rank) continue;
-                    all.push_back(make_int2(u, v));
-                }
-            }
-            w.count = (long long)all.size() - w.offset;
-            if (w.count) h->work.push_back(w);
+            unscreened += w.total;
+            if (w.items) all.push_back(w);
         }
-    h->nquart = (long long)all.size();
-    h->nquart_unscreened = unscreened;
-    PG_CUDA(upload(h->d_quart, all, h->stream));
+    if (all.size() > 64) return fail(PATGPU_ESTATE, "too many classes");
+    for (size_t k = 0; k < all.size(); ++k) {
+        EriArgs a = class_args(h, all[k], MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
+        long long blocks = std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
+        count_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, h->stream>>>(
+            a, dcnt.as<unsigned long long>() + k);
+    }
+    PG_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> cnt(64, 0);
+    PG_CUDA(cudaMemcpyAsync(cnt.data(), dcnt.p, sizeof(unsigned long long) * 64, cudaMemcpyDeviceToHost, h->stream));
     PG_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t k = 0; k < all.size(); ++k) {
+        all[k].count = (long long)cnt[k];
+        owned += all[k].count;
+        if (all[k].count) h->work.push_back(all[k]);
+    }
+    h->nquart = owned;
+    h->nquart_unscreened = unscreened;
     return 0;
 }
 
@@ -395,8 +466,9 @@ static int tune_variants(patgpu_basis *h)
     PG_CUDA(cudaEventCreate(&e0));
     PG_CUDA(cudaEventCreate(&e1));
     for (auto &w : h->work) {
-        a.quart = h->d_quart.as<int2>() + w.offset;
-        a.nquart = w.count;
+        a = class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
+        a.D0 = h->d_D0.as<double>();
+        a.A0 = h->d_A0.as<double>();
         float best = 1e30f;
         for (int var = 0; var <= 2; ++var) {
             if (!eri_has_variant(w.la, w.lb, w.lc, w.ld, var)) continue;
@@ -477,9 +549,7 @@ static int launch_fock(patgpu_basis *h, int mode, cudaStream_t s)
     PG_CUDA(cudaEventRecord(h->ev0, s));
     int launches = 0;
     for (auto &w : h->work) {
-        a.quart = h->d_quart.as<int2>() + w.offset;
-        a.nquart = w.count;
-        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant));
+        PG_CUDA(launch_work(h, w, a, s));
         ++launches;
     }
     PG_CUDA(cudaEventRecord(h->ev1, s));
@@ -688,9 +758,7 @@ int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, 
     PG_CUDA(cudaEventRecord(h->ev0, s));
     int launches = 0;
     for (auto &w : h->work) {
-        a.quart = h->d_quart.as<int2>() + w.offset;
-        a.nquart = w.count;
-        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant));
+        PG_CUDA(launch_work(h, w, a, s));
         ++launches;
     }
     PG_CUDA(cudaEventRecord(h->ev1, s));
@@ -781,9 +849,7 @@ int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double 
     a.D0 = D;
     a.A0 = A;
     for (auto &w : h->work) {
-        a.quart = h->d_quart.as<int2>() + w.offset;
-        a.nquart = w.count;
-        PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant));
+        PG_CUDA(launch_work(h, w, a, s));
     }
     const long long no2 = (long long)n * (n + 1) / 2;
     finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(A, dG, n);
@@ -874,6 +940,36 @@ int patgpu_fp64_peak(double *tflops)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *tflops = 4.0 * 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+    return 0;
+}
+
+int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
+{
+    if (!h || !(tau_fp32 >= 0.0)) return fail(PATGPU_EINVAL, "bad mixed-precision threshold");
+    h->tau_mix = tau_fp32;
+    h->nquart_fp32 = 0;
+    if (tau_fp32 <= 0.0 || tau_fp32 <= h->tau) return 0;
+    DBuf dcnt;
+    PG_CUDA(dcnt.ensure(sizeof(unsigned long long)));
+    PG_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long), h->stream));
+    for (auto &w : h->work) {
+        EriArgs a = class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, tau_fp32);
+        long long blocks = std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
+        count_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, h->stream>>>(a,
+                                                                                     dcnt.as<unsigned long long>());
+    }
+    PG_CUDA(cudaGetLastError());
+    unsigned long long c = 0;
+    PG_CUDA(cudaMemcpyAsync(&c, dcnt.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    PG_CUDA(cudaStreamSynchronize(h->stream));
+    h->nquart_fp32 = (long long)c;
+    return 0;
+}
+
+int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32)
+{
+    if (!h || !n_fp32) return fail(PATGPU_EINVAL, "null argument");
+    *n_fp32 = h->nquart_fp32;
     return 0;
 }
 

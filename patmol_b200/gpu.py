@@ -67,6 +67,8 @@ def lib():
         L.patgpu_last_timing.argtypes = [H, dp, ip]
         L.patgpu_rys_host.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.patgpu_fp64_peak.argtypes = [dp]
+        L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
+        L.patgpu_mixed_stats.argtypes = [H, lp]
         _lib = L
     return _lib
 
@@ -186,6 +188,14 @@ class GpuBasis:
 
     def finish_gmatrix_device(self, dA_ptr: int, dG_ptr: int, stream: int):
         _check(lib().patgpu_finish_gmatrix_device(self.h, dA_ptr, dG_ptr, stream), "finish")
+
+    def set_mixed_precision(self, tau_fp32: float) -> int:
+        """FP32 arithmetic for quartets with Schwarz bound below tau_fp32
+        (FP64 accumulation); returns how many quartets run in FP32."""
+        _check(lib().patgpu_set_mixed_precision(self.h, float(tau_fp32)), "set_mixed_precision")
+        n = ctypes.c_longlong()
+        _check(lib().patgpu_mixed_stats(self.h, ctypes.byref(n)), "mixed_stats")
+        return n.value
 
     def stats(self):
         o = np.zeros(5, dtype=np.int64)
