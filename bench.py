@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", default="patgpu", choices=["patgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tau", type=float, default=1e-14)
+    ap.add_argument("--tau-fp32", type=float, default=1e-8,
+                    help="Schwarz bound below which the mixed-precision leg runs quartets in FP32")
     return ap.parse_args()
 
 
@@ -243,10 +245,33 @@ def main():
     e2e_ms = e2e_ev[0].elapsed_time(e2e_ev[1]) / a.steps
     clk = clocks.stop()
 
-    t = torch.tensor([step_ms, e2e_ms, kern_ms], dtype=torch.float64, device=dev)
+    # mixed-precision leg: the same Fock builds with FP32 arithmetic for the
+    # quartets whose Schwarz bound is below tau_fp32 (FP64 accumulation)
+    ref_G = Gd.clone()
+    nfp32 = G.set_mixed_precision(a.tau_fp32)
+    for _ in range(a.warmup):
+        step()
+    mx_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    for i in range(a.steps):
+        flush.fill_(float(i))
+        mx_ev[i][0].record(stream)
+        step()
+        mx_ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    mixed_ms = sum(e0.elapsed_time(e1) for e0, e1 in mx_ev) / a.steps
+    dG = (Gd - ref_G).abs().max().item()
+    G.set_mixed_precision(0.0)
+    nfp32_t = torch.tensor([float(nfp32)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(nfp32_t)
+
+    t = torch.tensor([step_ms, e2e_ms, kern_ms, mixed_ms, dG], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms, e2e_ms, kern_ms = (float(x) for x in t.tolist())
+    step_ms, e2e_ms, kern_ms, mixed_ms, dG = (float(x) for x in t.tolist())
 
     line = None
     if rank == 0:
@@ -276,6 +301,9 @@ def main():
                          "peak_source": "measured FP64 FMA probe (patgpu_fp64_peak), this GPU, this run",
                          "algorithmic_flops_per_step": my_flops,
                          "kernel_ms_per_step": kern_ms},
+            "mixed": {"tau_fp32": a.tau_fp32, "fp32_quartets": int(nfp32_t.item()),
+                      "ms_per_step": mixed_ms, "speedup_vs_fp64": step_ms / mixed_ms,
+                      "max_abs_dG_vs_fp64": dG},
             "gpu_launches": launches,
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
