@@ -151,6 +151,26 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
                    const double *charge, const double *xyz, int skipcen, double *S, double *T,
                    double *H, double *Hdpm);
 
+/* Nuclear gradient of the closed-shell SCF energy (no counterpart in the
+ * reference, which has no gradients):
+ *   E = 2 tr(P H) + tr(P G[P]) + E_nuc,  H -= V_DPM when with_dpm,
+ * at a converged half density P (P = C_occ C_occ^T, packed lower triangle)
+ * and its energy-weighted density W = sum_occ e_i c_i c_i^T (packed, may be
+ * NULL when PATGPU_GRAD_1E is not asked for).  grad[3*ncen] (x, y, z per
+ * centre, ghost and positron centres included) is overwritten with the sum
+ * of the parts selected by the mask: PATGPU_GRAD_2E (derivative ERIs
+ * contracted with the density products on the GPU, over this handle's
+ * screened quartets -- with a rank split, only this rank's share),
+ * PATGPU_GRAD_1E (overlap/Pulay, kinetic, nuclear attraction including the
+ * moving charges, and DPM when with_dpm; GPU) and PATGPU_GRAD_NUC (nuclear
+ * repulsion over centre pairs whose charge product is non-zero; host). */
+#define PATGPU_GRAD_2E 1
+#define PATGPU_GRAD_1E 2
+#define PATGPU_GRAD_NUC 4
+#define PATGPU_GRAD_ALL 7
+int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,
+                        double *grad);
+
 /* Mixed precision (no counterpart in the reference, which is FP64
  * throughout): quartets whose Schwarz bound Q_ab Q_cd lies between the
  * screening threshold and tau_fp32 are computed with FP32 recursion,

@@ -200,6 +200,20 @@ class Basis:
                     skipcen=self.ncen)
         return out
 
+    def with_coords(self, coords) -> "Basis":
+        """The same basis with every centre at new coordinates (ncen x 3);
+        shells move with their centres (set_center_position, basis.c:163-166)."""
+        shells = [Shell(l=s.l, cen=s.cen, alpha=s.alpha, coef=s.coef, nst=s.nst) for s in self.shells]
+        return Basis(charges=self.charges.copy(), coords=np.array(coords, dtype=np.float64).reshape(-1, 3),
+                     shells=shells, raw=list(self.raw), nelec=self.nelec, mult=self.mult, maxit=self.maxit,
+                     eps=self.eps, dpm=self.dpm, accel=self.accel, guess=self.guess, ffc=self.ffc,
+                     skipcen=self.skipcen)
+
+    def displaced(self, center: int, dim: int, delta: float) -> "Basis":
+        xyz = self.coords.copy()
+        xyz[center, dim] += delta
+        return self.with_coords(xyz)
+
     def is_uhf(self) -> bool:
         """patmol.c:18: RHF iff the electron count is even and mult == 1."""
         return not (self.nelec % 2 == 0 and self.mult == 1)

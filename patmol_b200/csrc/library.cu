@@ -14,6 +14,7 @@
 
 #include "../../include/patgpu.h"
 #include "eri.cuh"
+#include "eri_grad.cuh"
 #include "onebody.cuh"
 #include "rys_table.h"
 
@@ -133,9 +134,12 @@ struct patgpu_basis {
     std::vector<int> psa, psb, pfa, pfb, pcls, pstart, pnum;
     std::vector<double> pax, pay, paz, pabx, paby, pabz, Q;
     std::vector<double> pp_p, pp_px, pp_py, pp_pz, pp_K, pp_cut;
+    std::vector<int> pca, pcb;        // centres of the two shells (gradient)
+    std::vector<double> pp_ea;        // exponent of the first shell's primitive (gradient)
     std::vector<int> class_begin;   // pairs of class c: [class_begin[c], class_begin[c+1])
     pg::DBuf d_psa, d_psb, d_pfa, d_pfb, d_pax, d_pay, d_paz, d_pabx, d_paby, d_pabz, d_pstart, d_pnum;
     pg::DBuf d_pp_p, d_pp_px, d_pp_py, d_pp_pz, d_pp_K, d_pp_cut, d_Q;
+    pg::DBuf d_pca, d_pcb, d_pp_ea;
     // quartets
     std::vector<pg::ClassWork> work;
     long long nquart = 0, nquart_unscreened = 0;
@@ -198,6 +202,7 @@ static int build_pairs(patgpu_basis *h)
     h->pstart.clear(); h->pnum.clear(); h->pax.clear(); h->pay.clear(); h->paz.clear();
     h->pabx.clear(); h->paby.clear(); h->pabz.clear();
     h->pp_p.clear(); h->pp_px.clear(); h->pp_py.clear(); h->pp_pz.clear(); h->pp_K.clear(); h->pp_cut.clear();
+    h->pca.clear(); h->pcb.clear(); h->pp_ea.clear();
     h->class_begin.assign(11, 0);
     for (auto &x : t) h->class_begin[x.cls + 1]++;
     for (int c = 0; c < 10; ++c) h->class_begin[c + 1] += h->class_begin[c];
@@ -210,6 +215,8 @@ static int build_pairs(patgpu_basis *h)
         h->pfa.push_back(h->off[x.a]);
         h->pfb.push_back(h->off[x.b]);
         h->pcls.push_back(x.cls);
+        h->pca.push_back(h->cen[x.a]);
+        h->pcb.push_back(h->cen[x.b]);
         h->pax.push_back(A[0]); h->pay.push_back(A[1]); h->paz.push_back(A[2]);
         h->pabx.push_back(AB[0]); h->paby.push_back(AB[1]); h->pabz.push_back(AB[2]);
         h->pstart.push_back((int)h->pp_p.size());
@@ -224,6 +231,7 @@ static int build_pairs(patgpu_basis *h)
                 h->pp_pz.push_back((ea * A[2] + eb * B[2]) / p);
                 h->pp_cut.push_back(s / p);
                 h->pp_K.push_back(h->co[i] * h->co[j] * s / p);
+                h->pp_ea.push_back(ea);
                 ++np;
             }
         h->pnum.push_back(np);
@@ -236,6 +244,7 @@ static int build_pairs(patgpu_basis *h)
     UP(d_pstart, pstart); UP(d_pnum, pnum);
     UP(d_pp_p, pp_p); UP(d_pp_px, pp_px); UP(d_pp_py, pp_py); UP(d_pp_pz, pp_pz); UP(d_pp_K, pp_K);
     UP(d_pp_cut, pp_cut);
+    UP(d_pca, pca); UP(d_pcb, pcb); UP(d_pp_ea, pp_ea);
 #undef UP
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(PATGPU_ECUDA, "pair upload: %s", cudaGetErrorString(e));
@@ -619,6 +628,60 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
     if (two)
         for (size_t i = 0; i < no2; ++i) G1[i] += h->h_stage[no2 + i];
     return 0;
+}
+
+// Two-electron gradient part: packed half density P, grad[3 ncen] += .
+static int grad_2e(patgpu_basis *h, const double *P, double *grad)
+{
+    int rc = ensure_work(h, false);
+    if (rc) return rc;
+    const size_t nn = (size_t)h->n * h->n, no2 = (size_t)h->n * (h->n + 1) / 2;
+    cudaStream_t s = h->stream;
+    PG_CUDA(cudaMemcpyAsync(h->d_Pk0.p, P, sizeof(double) * no2, cudaMemcpyHostToDevice, s));
+    unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(h->d_Pk0.as<double>(), h->d_D0.as<double>(),
+                                                                    h->n);
+    DBuf dg;
+    const size_t ng = 3 * (size_t)h->ncen;
+    PG_CUDA(dg.ensure(sizeof(double) * ng));
+    PG_CUDA(cudaMemsetAsync(dg.p, 0, sizeof(double) * ng, s));
+    GradArgs ga{};
+    ga.ca = h->d_pca.as<int>();
+    ga.cb = h->d_pcb.as<int>();
+    ga.ea = h->d_pp_ea.as<double>();
+    ga.grad = dg.as<double>();
+    for (const auto &w : h->work) {
+        EriArgs a = class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
+        a.D0 = h->d_D0.as<double>();
+        ga.la = w.la;
+        ga.lb = w.lb;
+        ga.lc = w.lc;
+        ga.ld = w.ld;
+        PG_CUDA(launch_eri_grad(a, ga, s, h->num_sms));
+    }
+    std::vector<double> hg(ng);
+    PG_CUDA(cudaMemcpyAsync(hg.data(), dg.p, sizeof(double) * ng, cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    for (size_t k = 0; k < ng; ++k) grad[k] += hg[k];
+    return 0;
+}
+
+// Nuclear repulsion over centre pairs with a non-zero charge product (the
+// rule the energy uses; a ghost centre may coincide with the positron).
+static void grad_nuc(const patgpu_basis *h, double *grad)
+{
+    for (int i = 0; i < h->ncen; ++i)
+        for (int j = 0; j < i; ++j) {
+            const double qq = h->q[i] * h->q[j];
+            if (qq == 0.0) continue;
+            const double d[3] = {h->xyz[3 * i] - h->xyz[3 * j], h->xyz[3 * i + 1] - h->xyz[3 * j + 1],
+                                 h->xyz[3 * i + 2] - h->xyz[3 * j + 2]};
+            const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            const double f = qq / (r2 * std::sqrt(r2));
+            for (int k = 0; k < 3; ++k) {
+                grad[3 * i + k] -= f * d[k];
+                grad[3 * j + k] += f * d[k];
+            }
+        }
 }
 
 }  // namespace pg
@@ -1038,6 +1101,30 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
     if (rc) return rc;
     return run_oneints(nshell, l, cen, off, nst, prim_off, alpha, coef, ncen, charge, xyz, skipcen, n, S, T, H, Hdpm,
                        nullptr);
+}
+
+int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,
+                        double *grad)
+{
+    if (!h || !P || !grad || parts < 0 || parts > PATGPU_GRAD_ALL)
+        return fail(PATGPU_EINVAL, "patgpu_rhf_gradient: bad argument");
+    if ((parts & PATGPU_GRAD_1E) && !W) return fail(PATGPU_EINVAL, "patgpu_rhf_gradient: the 1e part needs W");
+    const size_t ng = 3 * (size_t)h->ncen;
+    std::fill(grad, grad + ng, 0.0);
+    if (parts & PATGPU_GRAD_2E) {
+        int rc = grad_2e(h, P, grad);
+        if (rc) return rc;
+    }
+    if (parts & PATGPU_GRAD_1E) {
+        std::vector<double> g1(ng, 0.0);
+        int rc = run_onebody_grad(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
+                                  h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n, P,
+                                  W, with_dpm, g1.data(), h->stream);
+        if (rc) return rc;
+        for (size_t k = 0; k < ng; ++k) grad[k] += g1[k];
+    }
+    if (parts & PATGPU_GRAD_NUC) grad_nuc(h, grad);
+    return 0;
 }
 
 int patgpu_dpm(patgpu_handle h, double *H)

@@ -15,6 +15,14 @@ int run_oneints(int nsh, const int *l, const int *cen, const int *off, const int
                 const double *al, const double *co, int ncen, const double *q, const double *xyz, int skipcen,
                 int n, double *S, double *T, double *H, double *Hdpm, cudaStream_t stream);
 
+// Nuclear gradient of the one-body energy terms 2 tr(P H) - 2 tr(W S)
+// (H -= V_DPM when with_dpm) for the packed half density P and
+// energy-weighted density W (W may be NULL: no overlap term).  grad[3 ncen]
+// is overwritten (host buffer).
+int run_onebody_grad(int nsh, const int *l, const int *cen, const int *off, const int *nst, const int *poff,
+                     const double *al, const double *co, int ncen, const double *q, const double *xyz, int skipcen,
+                     int n, const double *P, const double *W, int with_dpm, double *grad, cudaStream_t stream);
+
 int fail(int code, const char *fmt, ...);
 
 }  // namespace pg

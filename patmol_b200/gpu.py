@@ -69,6 +69,7 @@ def lib():
         L.patgpu_fp64_peak.argtypes = [dp]
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_mixed_stats.argtypes = [H, lp]
+        L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
         _lib = L
     return _lib
 
@@ -188,6 +189,23 @@ class GpuBasis:
 
     def finish_gmatrix_device(self, dA_ptr: int, dG_ptr: int, stream: int):
         _check(lib().patgpu_finish_gmatrix_device(self.h, dA_ptr, dG_ptr, stream), "finish")
+
+    GRAD_2E, GRAD_1E, GRAD_NUC, GRAD_ALL = 1, 2, 4, 7
+
+    def rhf_gradient(self, P, W=None, parts: int = 7, with_dpm: bool = False):
+        """Nuclear gradient (ncen x 3) of E = 2 tr(PH) + tr(P G[P]) + E_nuc at
+        the packed half density P and energy-weighted density W; parts is a
+        mask of GRAD_2E / GRAD_1E / GRAD_NUC (patgpu_rhf_gradient)."""
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        null = ctypes.POINTER(ctypes.c_double)()
+        Wp = null
+        if W is not None:
+            W = np.ascontiguousarray(W, dtype=np.float64)
+            Wp = _p(W)
+        g = np.zeros(3 * self.basis.ncen)
+        _check(lib().patgpu_rhf_gradient(self.h, _p(P), Wp, int(parts), int(bool(with_dpm)), _p(g)),
+               "patgpu_rhf_gradient")
+        return g.reshape(-1, 3)
 
     def set_mixed_precision(self, tau_fp32: float) -> int:
         """FP32 arithmetic for quartets with Schwarz bound below tau_fp32
