@@ -36,6 +36,14 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 functions), RHF Fock build"
 
+# DRAM bytes (read + write) of the 55 class kernels of one Fock build of this
+# workload, from one ncu capture of dram__bytes_read.sum and
+# dram__bytes_write.sum (cold caches per launch); summarised with its command
+# in profiles/fock_build_water_spdf_positron_launches.md.
+STEP_DRAM_BYTES = 163.7e6
+STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 55 class kernels of one "
+                    "Fock build (37.9 MB read, 125.8 MB write, mostly local-memory write-back of three f classes)")
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -297,7 +305,8 @@ def main():
                     "h2d_bytes_per_step": no2 * 8, "d2h_bytes_per_step": no2 * 8,
                     "path": "pinned P -> patgpu_rhf_accumulate_device -> patgpu_finish_gmatrix_device -> pinned G"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None, "traffic": STEP_DRAM_BYTES,
+                         "traffic_source": STEP_DRAM_SOURCE,
                          "peak_source": "measured FP64 FMA probe (patgpu_fp64_peak), this GPU, this run",
                          "algorithmic_flops_per_step": my_flops,
                          "kernel_ms_per_step": kern_ms},
