@@ -38,8 +38,8 @@ WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 function
 
 # DRAM bytes (read + write) of the 55 class kernels of one Fock build of this
 # workload, from one ncu capture of dram__bytes_read.sum and
-# dram__bytes_write.sum (cold caches per launch); summarised with its command
-# in profiles/fock_build_water_spdf_positron_launches.md.
+# dram__bytes_write.sum (cold caches per launch); the capture's command and
+# per-kernel figures are kept with the other ncu summaries under profiles/.
 STEP_DRAM_BYTES = 163.7e6
 STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 55 class kernels of one "
                     "Fock build (37.9 MB read, 125.8 MB write, mostly local-memory write-back of three f classes)")
