@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--tau", type=float, default=1e-14)
     ap.add_argument("--tau-fp32", type=float, default=1e-8,
                     help="Schwarz bound below which the mixed-precision leg runs quartets in FP32")
+    ap.add_argument("--batch-molecules", type=int, default=32,
+                    help="molecules in the batched (lock-step, graph-captured) leg; 0 skips it")
     return ap.parse_args()
 
 
@@ -155,6 +157,61 @@ def run_reference_arm(a):
             "impl": "reference", "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": res["value"], "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+# --------------------------------------------------------------- batched
+def batched_leg(a, torch, stream, nmol: int):
+    """Lock-step Fock builds of many molecules as one CUDA graph (patgpu_batch)
+    against the same builds launched molecule by molecule, FP64 and mixed."""
+    import numpy as np
+    from patmol_b200 import configs, gpu
+    rng = np.random.default_rng(77)
+    sizes = rng.integers(3, 9, size=nmol)          # 3..8 atoms, uniform
+    bases = [configs.organic_basis(int(k), 1000 + i, with_f=False) for i, k in enumerate(sizes)]
+    gbs = [gpu.GpuBasis(bb, schwarz_tau=a.tau) for bb in bases]
+    batch = gpu.GpuBatch(gbs)
+    Ps = [np.random.default_rng(2000 + i).normal(scale=0.05, size=g.no2) for i, g in enumerate(gbs)]
+    G64 = batch.rhf_form_gmatrix(Ps)                # loads P into the batch buffers, captures the graph
+    sh = stream.cuda_stream
+    bufs = [batch.buffers(m) for m in range(nmol)]
+
+    def timed(fn, reps):
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def sequential():
+        for g, (dP, dG) in zip(gbs, bufs):
+            g.rhf_gmatrix_device(dP, dG, sh)
+
+    reps = max(1, min(a.steps, 5))
+    t_graph = timed(lambda: batch.launch(sh), reps)
+    t_seq = timed(sequential, reps)
+    st = batch.stats()
+    batch.set_mixed_precision(a.tau_fp32)
+    Gmx = batch.rhf_form_gmatrix(Ps)
+    t_mixed = timed(lambda: batch.launch(sh), reps)
+    stm = batch.stats()
+    dG = max(float(np.abs(x - y).max()) for x, y in zip(Gmx, G64))
+    batch.close()
+    for g in gbs:
+        g.close()
+    q = st["quartets"]
+    return {"workload": f"{nmol} seeded organic molecules (C/N/O/H walk), 3-8 atoms uniform, config-0 "
+                        "s/p/d basis, RHF Fock build of every molecule per step",
+            "molecules": nmol, "basis_functions": int(sum(bb.norb for bb in bases)), "quartets": q,
+            "graph_nodes": st["graph_nodes"],
+            "ms_per_step_graph": t_graph, "ms_per_step_sequential": t_seq,
+            "quartets_per_s_graph": q / (t_graph * 1e-3), "speedup_graph_vs_sequential": t_seq / t_graph,
+            "mixed": {"tau_fp32": a.tau_fp32, "fp32_quartets": stm["fp32_quartets"], "ms_per_step": t_mixed,
+                      "speedup_vs_fp64_graph": t_graph / t_mixed, "max_abs_dG_vs_fp64": dG}}
 
 
 # ------------------------------------------------------------------- GPU
@@ -316,6 +373,8 @@ def main():
             "gpu_launches": launches,
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
+        if world == 1 and a.batch_molecules > 0:
+            line["batched"] = batched_leg(a, torch, stream, a.batch_molecules)
         if world == 1 and not a.no_cpu_baseline:
             res, err = reference_fock(2, 1)
             line["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}

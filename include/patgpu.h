@@ -171,6 +171,29 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
 int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,
                         double *grad);
 
+/* Batches (no counterpart in the reference, which runs one molecule per
+ * process): many molecules advanced in lock step.  A batch holds the
+ * molecules' handles (which must outlive it and must not be used
+ * elsewhere while a batch launch runs: the batch uses their work buffers)
+ * and, per molecule, packed device buffers dP and dG.  patgpu_batch_launch
+ * computes dG_m = G[dP_m] (RHF, overwritten) for every molecule as ONE
+ * CUDA graph launch on `stream`; the graph is captured on the first launch
+ * (after one plain build per molecule) and holds each molecule's class
+ * launches, spread over parallel capture streams.  patgpu_batch_rhf_gmatrix
+ * is the host-buffer form (G_m += G[P_m]).  Mixed precision is per
+ * molecule; patgpu_batch_set_mixed_precision sets it for all and drops the
+ * graph.  Stats: [0] molecules, [1] quartets, [2] FP32 quartets, [3]
+ * graph nodes.  Timing: nanoseconds of the last graph launch (events). */
+typedef struct patgpu_batch_s *patgpu_batch;
+int patgpu_batch_create(int nmol, const patgpu_handle *mols, patgpu_batch *out);
+int patgpu_batch_destroy(patgpu_batch b);
+int patgpu_batch_buffers(patgpu_batch b, int m, double **dP, double **dG);
+int patgpu_batch_set_mixed_precision(patgpu_batch b, double tau_fp32);
+int patgpu_batch_launch(patgpu_batch b, void *stream);
+int patgpu_batch_rhf_gmatrix(patgpu_batch b, const double *const *P, double *const *G);
+int patgpu_batch_stats(patgpu_batch b, long long *out4);
+int patgpu_batch_last_timing(patgpu_batch b, double *kernel_ns);
+
 /* Mixed precision (no counterpart in the reference, which is FP64
  * throughout): quartets whose Schwarz bound Q_ab Q_cd lies between the
  * screening threshold and tau_fp32 are computed with FP32 recursion,

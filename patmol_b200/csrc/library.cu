@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdarg>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1133,6 +1134,252 @@ int patgpu_dpm(patgpu_handle h, double *H)
     return run_oneints(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
                        h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n, nullptr,
                        nullptr, nullptr, H, h->stream);
+}
+
+
+}  // extern "C"
+
+// ================================================================ batches
+// Many molecules advanced together: one CUDA graph holds every molecule's
+// Fock build (density unpack, accumulator clear, its quartet-class launches
+// in class order, the symmetrising finish), spread over kBatchStreams
+// capture streams so the small per-molecule grids run side by side.  The
+// graph is captured on the first launch (after one plain warm-up build per
+// molecule, which also configures every kernel) and replayed afterwards;
+// changing a molecule's mixed-precision threshold drops it.
+struct patgpu_batch_s {
+    std::vector<patgpu_basis *> mols;
+    std::unique_ptr<pg::DBuf[]> dP, dG;   // packed n(n+1)/2 per molecule
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> join;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int nodes = 0;
+    double last_ns = 0.0;
+    std::vector<double> stage;
+};
+
+namespace pg {
+
+constexpr int kBatchStreams = 8;
+
+static void batch_drop_graph(patgpu_batch_s *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->nodes = 0;
+}
+
+// One molecule's Fock build on stream s from the batch buffers.
+static int batch_enqueue(patgpu_batch_s *b, int m, cudaStream_t s)
+{
+    patgpu_basis *h = b->mols[m];
+    const size_t nn = (size_t)h->n * h->n;
+    const long long no2 = (long long)h->n * (h->n + 1) / 2;
+    unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(b->dP[m].as<double>(), h->d_D0.as<double>(),
+                                                                    h->n);
+    PG_CUDA(cudaMemsetAsync(h->d_A0.p, 0, sizeof(double) * nn, s));
+    EriArgs a = h->base_args();
+    a.mode = MODE_RHF;
+    a.D0 = h->d_D0.as<double>();
+    a.A0 = h->d_A0.as<double>();
+    for (const auto &w : h->work) PG_CUDA(launch_work(h, w, a, s));
+    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(h->d_A0.as<double>(), b->dG[m].as<double>(), h->n);
+    PG_CUDA(cudaGetLastError());
+    return 0;
+}
+
+static int batch_capture(patgpu_batch_s *b)
+{
+    const int nm = (int)b->mols.size();
+    // warm-up outside the capture: configures every kernel it will launch
+    for (int m = 0; m < nm; ++m) {
+        int rc = batch_enqueue(b, m, b->cs);
+        if (rc) return rc;
+    }
+    PG_CUDA(cudaStreamSynchronize(b->cs));
+    // heaviest molecules first, dealt round-robin over the capture streams
+    std::vector<int> order(nm);
+    for (int m = 0; m < nm; ++m) order[m] = m;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return b->mols[x]->nquart > b->mols[y]->nquart; });
+    PG_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    cudaError_t e = cudaEventRecord(b->fork, b->cs);
+    for (size_t k = 0; e == cudaSuccess && k < b->side.size(); ++k) e = cudaStreamWaitEvent(b->side[k], b->fork, 0);
+    for (int k = 0; e == cudaSuccess && !rc && k < nm; ++k) rc = batch_enqueue(b, order[k], b->side[k % b->side.size()]);
+    for (size_t k = 0; e == cudaSuccess && !rc && k < b->side.size(); ++k) {
+        e = cudaEventRecord(b->join[k], b->side[k]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cs, b->join[k], 0);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(b->cs, &g);
+    if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (rc) return rc;
+        return fail(PATGPU_ECUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    b->graph = g;
+    PG_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+    size_t nodes = 0;
+    PG_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+    b->nodes = (int)nodes;
+    return 0;
+}
+
+}  // namespace pg
+
+extern "C" {
+
+int patgpu_batch_create(int nmol, const patgpu_handle *mols, patgpu_batch *out)
+{
+    if (!out || nmol < 1 || !mols) return fail(PATGPU_EINVAL, "patgpu_batch_create: bad argument");
+    *out = nullptr;
+    for (int m = 0; m < nmol; ++m)
+        if (!mols[m]) return fail(PATGPU_EINVAL, "patgpu_batch_create: molecule %d has no handle", m);
+    auto *b = new patgpu_batch_s();
+    b->mols.assign(mols, mols + nmol);
+    b->dP.reset(new DBuf[nmol]);
+    b->dG.reset(new DBuf[nmol]);
+    auto bad = [&](const char *what) {
+        patgpu_batch_destroy(b);
+        return fail(PATGPU_ECUDA, "patgpu_batch_create: %s", what);
+    };
+    for (int m = 0; m < nmol; ++m) {
+        patgpu_basis *h = mols[m];
+        const size_t no2 = (size_t)h->n * (h->n + 1) / 2;
+        if (ensure_work(h, false) || b->dP[m].ensure(sizeof(double) * no2) != cudaSuccess ||
+            b->dG[m].ensure(sizeof(double) * no2) != cudaSuccess ||
+            cudaMemset(b->dP[m].p, 0, sizeof(double) * no2) != cudaSuccess)
+            return bad("device buffers");
+    }
+    if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return bad("streams/events");
+    const int ns = std::min(kBatchStreams, nmol);
+    for (int k = 0; k < ns; ++k) {
+        cudaStream_t s = nullptr;
+        cudaEvent_t ev = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return bad("streams");
+        b->side.push_back(s);
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return bad("events");
+        b->join.push_back(ev);
+    }
+    *out = b;
+    return 0;
+}
+
+int patgpu_batch_destroy(patgpu_batch b)
+{
+    if (!b) return 0;
+    if (b->cs) cudaStreamSynchronize(b->cs);
+    batch_drop_graph(b);
+    for (auto s : b->side) cudaStreamDestroy(s);
+    for (auto e : b->join) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->cs) cudaStreamDestroy(b->cs);
+    delete b;
+    return 0;
+}
+
+int patgpu_batch_buffers(patgpu_batch b, int m, double **dP, double **dG)
+{
+    if (!b || m < 0 || m >= (int)b->mols.size() || !dP || !dG) return fail(PATGPU_EINVAL, "bad batch buffer request");
+    *dP = b->dP[m].as<double>();
+    *dG = b->dG[m].as<double>();
+    return 0;
+}
+
+int patgpu_batch_set_mixed_precision(patgpu_batch b, double tau_fp32)
+{
+    if (!b) return fail(PATGPU_EINVAL, "null batch");
+    for (auto *h : b->mols) {
+        int rc = patgpu_set_mixed_precision(h, tau_fp32);
+        if (rc) return rc;
+    }
+    batch_drop_graph(b);
+    return 0;
+}
+
+int patgpu_batch_launch(patgpu_batch b, void *stream)
+{
+    if (!b) return fail(PATGPU_EINVAL, "null batch");
+    if (!b->exec) {
+        int rc = batch_capture(b);
+        if (rc) return rc;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    PG_CUDA(cudaEventRecord(b->ev0, s));
+    PG_CUDA(cudaGraphLaunch(b->exec, s));
+    PG_CUDA(cudaEventRecord(b->ev1, s));
+    return 0;
+}
+
+int patgpu_batch_rhf_gmatrix(patgpu_batch b, const double *const *P, double *const *G)
+{
+    if (!b || !P || !G) return fail(PATGPU_EINVAL, "patgpu_batch_rhf_gmatrix: null argument");
+    const int nm = (int)b->mols.size();
+    size_t tot = 0;
+    for (int m = 0; m < nm; ++m) {
+        if (!P[m] || !G[m]) return fail(PATGPU_EINVAL, "patgpu_batch_rhf_gmatrix: molecule %d has no matrix", m);
+        tot += (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
+    }
+    if (!b->exec) {
+        int rc = batch_capture(b);
+        if (rc) return rc;
+    }
+    for (int m = 0; m < nm; ++m) {
+        const size_t no2 = (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
+        PG_CUDA(cudaMemcpyAsync(b->dP[m].p, P[m], sizeof(double) * no2, cudaMemcpyHostToDevice, b->cs));
+    }
+    int rc = patgpu_batch_launch(b, b->cs);
+    if (rc) return rc;
+    b->stage.resize(tot);
+    size_t o = 0;
+    for (int m = 0; m < nm; ++m) {
+        const size_t no2 = (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
+        PG_CUDA(cudaMemcpyAsync(b->stage.data() + o, b->dG[m].p, sizeof(double) * no2, cudaMemcpyDeviceToHost, b->cs));
+        o += no2;
+    }
+    PG_CUDA(cudaStreamSynchronize(b->cs));
+    o = 0;
+    for (int m = 0; m < nm; ++m) {
+        const size_t no2 = (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
+        for (size_t k = 0; k < no2; ++k) G[m][k] += b->stage[o + k];
+        o += no2;
+    }
+    return 0;
+}
+
+int patgpu_batch_stats(patgpu_batch b, long long *out4)
+{
+    if (!b || !out4) return fail(PATGPU_EINVAL, "null argument");
+    long long q = 0, q32 = 0;
+    for (auto *h : b->mols) {
+        q += h->nquart;
+        q32 += h->nquart_fp32;
+    }
+    out4[0] = (long long)b->mols.size();
+    out4[1] = q;
+    out4[2] = q32;
+    out4[3] = b->nodes;
+    return 0;
+}
+
+int patgpu_batch_last_timing(patgpu_batch b, double *ns)
+{
+    if (!b || !ns) return fail(PATGPU_EINVAL, "null argument");
+    float ms = 0.f;
+    PG_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    *ns = ms * 1e6;
+    return 0;
 }
 
 }  // extern "C"

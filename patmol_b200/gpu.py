@@ -70,6 +70,14 @@ def lib():
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_mixed_stats.argtypes = [H, lp]
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.patgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(H), ctypes.POINTER(H)]
+        L.patgpu_batch_destroy.argtypes = [H]
+        L.patgpu_batch_buffers.argtypes = [H, ctypes.c_int, ctypes.POINTER(dp), ctypes.POINTER(dp)]
+        L.patgpu_batch_set_mixed_precision.argtypes = [H, ctypes.c_double]
+        L.patgpu_batch_launch.argtypes = [H, ctypes.c_void_p]
+        L.patgpu_batch_rhf_gmatrix.argtypes = [H, ctypes.POINTER(dp), ctypes.POINTER(dp)]
+        L.patgpu_batch_stats.argtypes = [H, lp]
+        L.patgpu_batch_last_timing.argtypes = [H, dp]
         _lib = L
     return _lib
 
@@ -231,6 +239,62 @@ class GpuBasis:
         n = ctypes.c_int()
         _check(lib().patgpu_last_timing(self.h, ctypes.byref(ns), ctypes.byref(n)), "patgpu_last_timing")
         return ns.value, n.value
+
+
+class GpuBatch:
+    """Lock-step Fock builds of many molecules as one CUDA graph
+    (patgpu_batch_*).  The GpuBasis objects must outlive the batch."""
+
+    def __init__(self, gpu_bases):
+        self.mols = list(gpu_bases)
+        arr = (ctypes.c_void_p * len(self.mols))(*[g.h for g in self.mols])
+        b = ctypes.c_void_p()
+        _check(lib().patgpu_batch_create(len(self.mols), arr, ctypes.byref(b)), "patgpu_batch_create")
+        self.b = b
+
+    def close(self):
+        if self.b:
+            lib().patgpu_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_mixed_precision(self, tau_fp32: float):
+        _check(lib().patgpu_batch_set_mixed_precision(self.b, float(tau_fp32)), "batch mixed precision")
+
+    def rhf_form_gmatrix(self, Ps):
+        """G_m = G[P_m] for every molecule (packed host arrays)."""
+        Ps = [np.ascontiguousarray(P, dtype=np.float64) for P in Ps]
+        Gs = [np.zeros(g.no2) for g in self.mols]
+        dp = ctypes.POINTER(ctypes.c_double)
+        pa = (dp * len(Ps))(*[_p(P) for P in Ps])
+        ga = (dp * len(Gs))(*[_p(G) for G in Gs])
+        _check(lib().patgpu_batch_rhf_gmatrix(self.b, pa, ga), "patgpu_batch_rhf_gmatrix")
+        return Gs
+
+    def buffers(self, m: int):
+        """Device addresses of molecule m's packed P and G buffers."""
+        dP = ctypes.POINTER(ctypes.c_double)()
+        dG = ctypes.POINTER(ctypes.c_double)()
+        _check(lib().patgpu_batch_buffers(self.b, m, ctypes.byref(dP), ctypes.byref(dG)), "batch buffers")
+        return ctypes.cast(dP, ctypes.c_void_p).value, ctypes.cast(dG, ctypes.c_void_p).value
+
+    def launch(self, stream: int):
+        _check(lib().patgpu_batch_launch(self.b, stream), "patgpu_batch_launch")
+
+    def stats(self):
+        o = np.zeros(4, dtype=np.int64)
+        _check(lib().patgpu_batch_stats(self.b, _p(o, ctypes.c_longlong)), "patgpu_batch_stats")
+        return dict(molecules=int(o[0]), quartets=int(o[1]), fp32_quartets=int(o[2]), graph_nodes=int(o[3]))
+
+    def last_timing_ns(self) -> float:
+        v = ctypes.c_double()
+        _check(lib().patgpu_batch_last_timing(self.b, ctypes.byref(v)), "patgpu_batch_last_timing")
+        return v.value
 
 
 def onebody(basis, want_sth=True, Hdpm=None):

@@ -20,7 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from .basis import Basis, pack, unpack
-from .gpu import GpuBasis
+from .gpu import GpuBasis, GpuBatch
 
 
 def nuclear_repulsion(basis: Basis) -> float:
@@ -55,73 +55,126 @@ def orthogonalizer(S: np.ndarray, smin: float = 1e-10) -> np.ndarray:
     return U[:, keep] / np.sqrt(s[keep])
 
 
-def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
-        maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8) -> RHFResult:
-    if basis.nelec % 2 or basis.mult != 1:
-        raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
-    gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
-    gb.two_electron_ints()
-    Sp, _, Hp = gb.one_electron_ints()
-    if dpm:
-        Hp = gb.dpm_ints(Hp)
-    n = basis.norb
-    nocc = basis.nelec // 2
-    S, H = unpack(Sp, n), unpack(Hp, n)
-    X = orthogonalizer(S)
-    enuc = nuclear_repulsion(basis)
+class _RHFState:
+    """One molecule's closed-shell iteration (host side of rhf_scf_update)."""
 
-    def diag(F):
-        e, V = np.linalg.eigh(X.T @ F @ X)
-        return e, X @ V
+    def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float):
+        if basis.nelec % 2 or basis.mult != 1:
+            raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
+        self.n = basis.norb
+        self.nocc = basis.nelec // 2
+        self.S, self.H = unpack(Sp, self.n), unpack(Hp, self.n)
+        self.X = orthogonalizer(self.S)
+        self.enuc = nuclear_repulsion(basis)
+        self.ndiis, self.conv = ndiis, conv
+        self.eps, C = self.diag(self.H)
+        self.P = C[:, :self.nocc] @ C[:, :self.nocc].T
+        self.fs, self.es = [], []
+        self.e_old = None
+        self.converged = False
+        self.it = 0
 
-    eps, C = diag(H)
-    P = C[:, :nocc] @ C[:, :nocc].T
-    fs, es = [], []
-    e_old = None
-    converged = False
-    it = 0
-    for it in range(1, maxit + 1):
-        G = unpack(gb.rhf_form_gmatrix(pack(P)), n)
-        F = H + G
-        energy = 2.0 * np.sum(P * H) + np.sum(P * G) + enuc
-        err = F @ P @ S - S @ P @ F
-        fs.append(F)
-        es.append(X.T @ err @ X)
-        fs, es = fs[-ndiis:], es[-ndiis:]
-        if len(fs) > 1:
-            m = len(fs)
+    def diag(self, F):
+        e, V = np.linalg.eigh(self.X.T @ F @ self.X)
+        return e, self.X @ V
+
+    def packed_density(self):
+        return pack(self.P)
+
+    def step(self, Gp):
+        """Consume G[P] of the current density; DIIS-extrapolated F gives the next P."""
+        self.it += 1
+        G = unpack(Gp, self.n)
+        F = self.H + G
+        energy = 2.0 * np.sum(self.P * self.H) + np.sum(self.P * G) + self.enuc
+        err = F @ self.P @ self.S - self.S @ self.P @ F
+        self.fs.append(F)
+        self.es.append(self.X.T @ err @ self.X)
+        self.fs, self.es = self.fs[-self.ndiis:], self.es[-self.ndiis:]
+        if len(self.fs) > 1:
+            m = len(self.fs)
             B = -np.ones((m + 1, m + 1))
             B[m, m] = 0.0
             for i in range(m):
                 for j in range(m):
-                    B[i, j] = np.sum(es[i] * es[j])
+                    B[i, j] = np.sum(self.es[i] * self.es[j])
             rhs = np.zeros(m + 1)
             rhs[m] = -1.0
             try:
                 c = np.linalg.solve(B, rhs)[:m]
-                F = sum(ci * Fi for ci, Fi in zip(c, fs))
+                F = sum(ci * Fi for ci, Fi in zip(c, self.fs))
             except np.linalg.LinAlgError:
                 pass
-        eps, C = diag(F)
-        P_new = C[:, :nocc] @ C[:, :nocc].T
-        dP = float(np.max(np.abs(P_new - P)))
-        P = P_new
-        if e_old is not None and abs(energy - e_old) < conv and float(np.max(np.abs(es[-1]))) < 1e-9 \
-                and dP < 1e-8:
-            converged = True
-            break
-        e_old = energy
-    # energy and orbitals of the final density
-    G = unpack(gb.rhf_form_gmatrix(pack(P)), n)
-    F = H + G
-    energy = 2.0 * np.sum(P * H) + np.sum(P * G) + enuc
-    eps, C = diag(F)
-    P = C[:, :nocc] @ C[:, :nocc].T
-    W = (C[:, :nocc] * eps[:nocc]) @ C[:, :nocc].T
+        self.eps, C = self.diag(F)
+        P_new = C[:, :self.nocc] @ C[:, :self.nocc].T
+        dP = float(np.max(np.abs(P_new - self.P)))
+        self.P = P_new
+        if self.e_old is not None and abs(energy - self.e_old) < self.conv and \
+                float(np.max(np.abs(self.es[-1]))) < 1e-9 and dP < 1e-8:
+            self.converged = True
+        self.e_old = energy
+
+    def finish(self, Gp) -> RHFResult:
+        """Energy and orbitals of the final density."""
+        G = unpack(Gp, self.n)
+        F = self.H + G
+        energy = 2.0 * np.sum(self.P * self.H) + np.sum(self.P * G) + self.enuc
+        eps, C = self.diag(F)
+        o = self.nocc
+        P = C[:, :o] @ C[:, :o].T
+        W = (C[:, :o] * eps[:o]) @ C[:, :o].T
+        return RHFResult(energy=float(energy), P=pack(P), W=pack(W), C=C, eps=eps, iterations=self.it,
+                         converged=self.converged, enuc=self.enuc)
+
+
+def _setup(gb: GpuBasis, dpm: bool):
+    gb.two_electron_ints()
+    Sp, _, Hp = gb.one_electron_ints()
+    if dpm:
+        Hp = gb.dpm_ints(Hp)
+    return Sp, Hp
+
+
+def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
+        maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8) -> RHFResult:
+    gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
+    Sp, Hp = _setup(gb, dpm)
+    st = _RHFState(basis, Sp, Hp, ndiis, conv)
+    while st.it < maxit and not st.converged:
+        st.step(gb.rhf_form_gmatrix(st.packed_density()))
+    res = st.finish(gb.rhf_form_gmatrix(st.packed_density()))
     if gpu is None:
         gb.close()
-    return RHFResult(energy=float(energy), P=pack(P), W=pack(W), C=C, eps=eps, iterations=it,
-                     converged=converged, enuc=enuc)
+    return res
+
+
+def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-12, maxit: int = 100,
+              schwarz_tau: float = 1e-14, ndiis: int = 8):
+    """Closed-shell SCF of many molecules in lock step: every iteration is one
+    batched Fock build (one CUDA graph over all molecules, patgpu_batch_*),
+    then each molecule's host step.  Converged molecules keep their density.
+    tau_fp32 > 0 runs quartets with Schwarz bound below it in FP32."""
+    gbs = [GpuBasis(b, schwarz_tau=schwarz_tau) for b in bases]
+    states = []
+    for b, gb in zip(bases, gbs):
+        Sp, Hp = _setup(gb, dpm)
+        states.append(_RHFState(b, Sp, Hp, ndiis, conv))
+    batch = GpuBatch(gbs)
+    if tau_fp32 > 0.0:
+        batch.set_mixed_precision(tau_fp32)
+    it = 0
+    while it < maxit and not all(st.converged for st in states):
+        it += 1
+        Gs = batch.rhf_form_gmatrix([st.packed_density() for st in states])
+        for st, G in zip(states, Gs):
+            if not st.converged:
+                st.step(G)
+    Gs = batch.rhf_form_gmatrix([st.packed_density() for st in states])
+    out = [st.finish(G) for st, G in zip(states, Gs)]
+    batch.close()
+    for gb in gbs:
+        gb.close()
+    return out
 
 
 def rhf_gradient(basis: Basis, res: RHFResult, dpm: bool = False, gpu: GpuBasis | None = None,
