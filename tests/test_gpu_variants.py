@@ -1,0 +1,37 @@
+"""Every kernel variant, forced for every class where it exists
+(PATGPU_VARIANT=lane|reg|smem), gives the oracle's G within 1e-11 on a
+65-function water basis whose shells cover all 55 quartet classes up to
+(ff|ff); the autotuner's own choice is checked the same way."""
+
+import numpy as np
+import pytest
+
+import patref
+
+from golden.make_golden import seeded_density  # noqa: E402
+from test_gpu_gradient import small_water  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+gpu = pytest.importorskip("patmol_b200.gpu")
+
+
+@pytest.fixture(scope="module")
+def water_ref():
+    b = small_water(f_on_o=True)
+    P = seeded_density(b.norb, 21)
+    return b, P, patref.Oracle(b).gmat(P)
+
+
+@pytest.mark.parametrize("variant", ["lane", "reg", "smem", None])
+def test_variant_matches_oracle(water_ref, variant, monkeypatch):
+    b, P, ref = water_ref
+    if variant is None:
+        monkeypatch.delenv("PATGPU_VARIANT", raising=False)
+    else:
+        monkeypatch.setenv("PATGPU_VARIANT", variant)
+    g = gpu.GpuBasis(b)
+    assert len(g.class_counts()) == 55
+    G = g.rhf_form_gmatrix(P)
+    assert np.abs(G - ref).max() < 1e-11
+    g.close()
