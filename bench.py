@@ -57,6 +57,15 @@ def parse():
                     help="Schwarz bound below which the mixed-precision leg runs quartets in FP32")
     ap.add_argument("--batch-molecules", type=int, default=32,
                     help="molecules in the batched (lock-step, graph-captured) leg; 0 skips it")
+    ap.add_argument("--alkane-carbons", type=int, default=12)
+    ap.add_argument("--scf-iters", type=int, default=3,
+                    help="alkane_dpm: SCF iterations before the gradient (timing; the converged "
+                         "finite-difference check runs at C3H8 size in the GPU tests)")
+    ap.add_argument("--workload", default="water_positron",
+                    choices=["water_positron", "organic40", "alkane_dpm"],
+                    help="water_positron: the headline line; organic40: FP64 vs mixed Fock build of the "
+                         "40-atom organic molecule; alkane_dpm: SCF and analytic gradient of C12H26 with "
+                         "positron shells and DPM (one GPU)")
     return ap.parse_args()
 
 
@@ -214,6 +223,120 @@ def batched_leg(a, torch, stream, nmol: int):
                       "speedup_vs_fp64_graph": t_graph / t_mixed, "max_abs_dG_vs_fp64": dG}}
 
 
+# ------------------------------------------------------ other workloads
+def _timed_builds(torch, stream, G, P, Gd, reps):
+    """Device-timed Fock builds (ms each) through patgpu_rhf_gmatrix_device."""
+    sh = stream.cuda_stream
+    G.rhf_gmatrix_device(P.data_ptr(), Gd.data_ptr(), sh)
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        G.rhf_gmatrix_device(P.data_ptr(), Gd.data_ptr(), sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return sum(out) / len(out)
+
+
+def organic40_leg(a, torch, stream):
+    """Config: 40-atom seeded organic molecule (C/N/O/H walk), s/p/d/f basis;
+    FP64 vs mixed (Schwarz bound < tau_fp32 in FP32) Fock builds at the core
+    Hamiltonian guess density, with the energy change tr(P dG)."""
+    import numpy as np
+    from patmol_b200 import configs, gpu, workload
+    from patmol_b200.basis import unpack
+    from patmol_b200.scf import orthogonalizer
+    t0 = time.time()
+    b = configs.organic_basis(40, 2, with_f=True)
+    G = gpu.GpuBasis(b, schwarz_tau=a.tau)
+    G.two_electron_ints()
+    t_setup = time.time() - t0
+    st = G.stats()
+    Sp, _, Hp = G.one_electron_ints()
+    n = b.norb
+    X = orthogonalizer(unpack(Sp, n))
+    e, V = np.linalg.eigh(X.T @ unpack(Hp, n) @ X)
+    C = X @ V
+    Pf = C[:, :b.nelec // 2] @ C[:, :b.nelec // 2].T
+    Pp = Pf[np.tril_indices(n)]
+    il = np.tril_indices(n)
+    w = np.where(il[0] == il[1], 1.0, 2.0)
+    P = torch.from_numpy(Pp.copy()).to("cuda")
+    Gd = torch.empty_like(P)
+    reps = max(1, min(a.steps, 1))
+    ms64 = _timed_builds(torch, stream, G, P, Gd, reps)
+    G64 = Gd.cpu().numpy()
+    nfp32 = G.set_mixed_precision(a.tau_fp32)
+    msmx = _timed_builds(torch, stream, G, P, Gd, reps)
+    Gmx = Gd.cpu().numpy()
+    flops = workload.fock_flops(G.class_counts(), "rhf")
+    kern_ns, _ = G.last_timing()
+    q = st["quartets"]
+    return {"metric": "ERI quartets/s (Fock build)", "value": q / (ms64 * 1e-3), "unit": "quartets/s",
+            "n_gpus": 1, "steps": reps, "warmup": 1, "ms_per_step": ms64, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "40-atom seeded organic molecule (C/N/O/H walk, seed 2), s/p/d/f "
+                                   "even-tempered basis, RHF Fock build at the core-Hamiltonian guess density",
+                       "basis_functions": n, "shells": b.nshell, "quartets": q,
+                       "quartets_unscreened": st["unscreened"], "schwarz_tau": a.tau,
+                       "setup_s": t_setup},
+            "roofline": {"bound": "fp64", "achieved": flops / (ms64 * 1e-3) / 1e12, "unit": "TFLOP/s",
+                         "peak": gpu.fp64_peak_tflops()},
+            "mixed": {"tau_fp32": a.tau_fp32, "fp32_quartets": nfp32, "ms_per_step": msmx,
+                      "speedup_vs_fp64": ms64 / msmx,
+                      "dE_fixed_density": float(np.sum(w * Pp * (Gmx - G64))),
+                      "max_abs_dG_vs_fp64": float(np.abs(Gmx - G64).max())}}
+
+
+def alkane_dpm_leg(a, torch, stream):
+    """Config: C12H26 (seeded jitter), s/p/d basis, ghost centroid with the
+    positron s/p/d shells and DPM on; converged SCF, then the analytic
+    gradient (derivative ERIs recomputed, not stored)."""
+    import numpy as np
+    from patmol_b200 import configs, gpu, scf
+    from patmol_b200.basis import Basis
+    sym, xyz = configs.alkane(a.alkane_carbons, 0)
+    mol = configs.molecule_basis(sym, xyz, with_f=False)
+    cen = xyz.mean(axis=0)
+    specs = [(r[1], r[2], r[3], r[4]) for r in mol.raw] + configs.ghost_shells(len(sym))
+    q = np.concatenate([mol.charges, [0.0]])
+    b = Basis.from_shell_list(q, np.vstack([xyz, cen[None, :]]), specs, nelec=mol.nelec, mult=1,
+                              dpm=1).dpm_augmented(cen)
+    t0 = time.time()
+    G = gpu.GpuBasis(b, schwarz_tau=a.tau)
+    t_setup = time.time() - t0
+    t0 = time.time()
+    res = scf.rhf(b, dpm=True, gpu=G, conv=1e-10, maxit=a.scf_iters)
+    t_scf = time.time() - t0
+    ns_fock, _ = G.last_timing()
+    torch.cuda.synchronize()
+    t0 = time.time()
+    g = G.rhf_gradient(res.P, res.W, parts=G.GRAD_ALL, with_dpm=True)
+    t_grad = time.time() - t0
+    t0 = time.time()
+    g2 = G.rhf_gradient(res.P, res.W, parts=G.GRAD_2E)
+    t_grad2e = time.time() - t0
+    st = G.stats()
+    torque = np.cross(b.coords, g).sum(axis=0)
+    return {"metric": "analytic gradient (s)", "value": t_grad, "unit": "s", "n_gpus": 1, "steps": 1,
+            "warmup": 0, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"C{a.alkane_carbons}H{2 * a.alkane_carbons + 2} (C-C 2.91, C-H 2.06 bohr, "
+                                   "seeded 0.05 bohr jitter), s/p/d basis, ghost centroid with positron s/p/d "
+                                   f"shells, DPM on, RHF; gradient at the density after {a.scf_iters} SCF "
+                                   "iterations (timing)",
+                       "basis_functions": b.norb, "shells": b.nshell, "quartets": st["quartets"],
+                       "quartets_unscreened": st["unscreened"], "schwarz_tau": a.tau, "setup_s": t_setup},
+            "scf": {"energy": res.energy, "iterations": res.iterations, "converged": res.converged,
+                    "seconds": t_scf, "last_fock_build_ms": ns_fock / 1e6},
+            "gradient": {"seconds_all_parts": t_grad, "seconds_two_electron": t_grad2e,
+                         "max_abs": float(np.abs(g).max()), "net_force": float(np.abs(g.sum(axis=0)).max()),
+                         "net_torque": float(np.abs(torque).max()),
+                         "positron_centre": [float(x) for x in g[b.skipcen]],
+                         "two_electron_share_max_abs": float(np.abs(g2).max())}}
+
+
 # ------------------------------------------------------------------- GPU
 def main():
     a = parse()
@@ -224,6 +347,13 @@ def main():
     import torch
     import torch.distributed as dist
     from patmol_b200 import configs, gpu, workload
+    if a.workload != "water_positron":
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        leg = organic40_leg if a.workload == "organic40" else alkane_dpm_leg
+        print(json.dumps(leg(a, torch, stream)))
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

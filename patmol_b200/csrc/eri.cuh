@@ -40,6 +40,9 @@ struct EriArgs {
     // least start_shell.
     int implicit;
     int u0, nu, v0, nv, same, rank, nranks, start_shell;
+    // compacted mode (implicit and klist set): item qi is class quartet
+    // klist[qi], already screened; no window test
+    const unsigned long long *klist;
     const double *Q;
     double tau_lo, tau_hi;
     int mode;
@@ -78,7 +81,7 @@ __device__ __forceinline__ bool eri_quartet_at(const EriArgs &a, long long qi, i
         ub = q.x;
         vk = q.y;
     } else {
-        const long long k = qi * a.nranks + a.rank;
+        const long long k = a.klist ? (long long)__ldg(a.klist + qi) : qi * a.nranks + a.rank;
         long long i, j;
         if (a.same) {
             i = (long long)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
@@ -93,11 +96,13 @@ __device__ __forceinline__ bool eri_quartet_at(const EriArgs &a, long long qi, i
         }
         ub = a.u0 + (int)i;
         vk = a.v0 + (int)j;
-        const double b = __ldg(a.Q + ub) * __ldg(a.Q + vk);
-        if (!(b >= a.tau_lo && b < a.tau_hi)) return false;
-        if (a.start_shell > 0 &&
-            max(max(a.pr.sa[ub], a.pr.sb[ub]), max(a.pr.sa[vk], a.pr.sb[vk])) < a.start_shell)
-            return false;
+        if (!a.klist) {
+            const double b = __ldg(a.Q + ub) * __ldg(a.Q + vk);
+            if (!(b >= a.tau_lo && b < a.tau_hi)) return false;
+            if (a.start_shell > 0 &&
+                max(max(a.pr.sa[ub], a.pr.sb[ub]), max(a.pr.sa[vk], a.pr.sb[vk])) < a.start_shell)
+                return false;
+        }
     }
     u = a.swap ? vk : ub;
     v = a.swap ? ub : vk;

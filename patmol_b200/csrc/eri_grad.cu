@@ -5,9 +5,10 @@
 // shared-memory Fock kernel.  Per quartet the team forms the weights
 // deg * Gamma * (component factors of basis.c:309-319) in shared memory;
 // per primitive quartet it evaluates the Rys rule, lanes j < 3n build the
-// 2-D recursion (rys.c:2269-2293) for one root and direction and transfer it
-// (rys.c:2295-2336) to the extended 1-D table I[a][b][c][d] with
-// a <= la+1, b <= lb+1, c <= lc+1, d <= ld; then every lane walks its
+// 2-D recursion (rys.c:2269-2293) for one root and direction in shared
+// memory, all lanes then transfer it (rys.c:2295-2336) to the extended 1-D
+// table I[a][b][c][d] with a <= la+1, b <= lb+1, c <= lc+1, d <= ld, one
+// table entry per lane at a time; then every lane walks its
 // Cartesian components and accumulates nine sums (centres A, B, C times
 // x, y, z).  The team reduces them and adds twelve numbers into the
 // gradient with FP64 atomics.  The class is a runtime argument: the
@@ -29,14 +30,15 @@ constexpr int kBlk = 128;
 
 struct GradDims {
     int la, lb, lc, ld, na, nb, nc, nd, ncart;
-    int nr, l12, l34, ea, eb, ec, ed, tsz;
+    int nr, l12, l34, ea, eb, ec, ed, tsz, gsz;
     int tq, nteam, rw, team;   // team: doubles of shared memory per team
 };
 
+// Lanes per team: the transfer and contraction phases spread over all of
+// them, so mid-size classes take whole warps and large ones a block.
 int tq_for(int ncart)
 {
-    const int t = ncart <= 300 ? 8 : ncart <= 700 ? 16 : ncart <= 1500 ? 32 : ncart <= 3000 ? 64 : 128;
-    return t;
+    return ncart <= 300 ? 32 : ncart <= 1500 ? 64 : 128;
 }
 
 GradDims grad_dims(int la, int lb, int lc, int ld)
@@ -53,30 +55,32 @@ GradDims grad_dims(int la, int lb, int lc, int ld)
     d.l34 = lc + ld + 1;
     d.ea = la + 2; d.eb = lb + 2; d.ec = lc + 2; d.ed = ld + 1;
     d.tsz = d.ea * d.eb * d.ec * d.ed;
+    d.gsz = (d.l12 + 1) * (d.l34 + 1);
     d.tq = tq_for(d.ncart);
     d.nteam = kBlk / d.tq;
     d.rw = (2 * d.nr + 1) / 2 * 2;
-    d.team = (d.rw + 3 * d.nr * d.tsz + d.ncart + 9 * d.tq + 1) / 2 * 2;
+    d.team = (d.rw + 3 * d.nr * d.gsz + 3 * d.nr * d.tsz + d.ncart + 9 * d.tq + 1) / 2 * 2;
     return d;
 }
 
-// 2-D recursion into G (row stride 8) for i <= l12, j <= l34.
-__device__ __forceinline__ void grad_vrr(double G[8][8], int l12, int l34, double g00, double B00, double B10,
+// 2-D recursion into G[i * W + j] (W = l34 + 1) for i <= l12, j <= l34.
+__device__ __forceinline__ void grad_vrr(double *G, int l12, int l34, double g00, double B00, double B10,
                                          double B01, double C, double Cp)
 {
-    G[0][0] = g00;
-    G[1][0] = C * g00;
-    for (int i = 1; i < l12; ++i) G[i + 1][0] = i * B10 * G[i - 1][0] + C * G[i][0];
+    const int W = l34 + 1;
+    G[0] = g00;
+    G[W] = C * g00;
+    for (int i = 1; i < l12; ++i) G[(i + 1) * W] = i * B10 * G[(i - 1) * W] + C * G[i * W];
     for (int j = 0; j < l34; ++j)
         for (int i = 0; i <= l12; ++i) {
-            double v = Cp * G[i][j];
-            if (j > 0) v = fma(j * B01, G[i][j - 1], v);
-            if (i > 0) v = fma(i * B00, G[i - 1][j], v);
-            G[i][j + 1] = v;
+            double v = Cp * G[i * W + j];
+            if (j > 0) v = fma(j * B01, G[i * W + j - 1], v);
+            if (i > 0) v = fma(i * B00, G[(i - 1) * W + j], v);
+            G[i * W + j + 1] = v;
         }
 }
 
-__global__ void __launch_bounds__(kBlk) eri_grad_kernel(const EriArgs args, const GradArgs ga, const GradDims dm)
+__global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, const GradArgs ga, const GradDims dm)
 {
     extern __shared__ double smem[];
     __shared__ int s_np[kBlk / 8];
@@ -87,7 +91,8 @@ __global__ void __launch_bounds__(kBlk) eri_grad_kernel(const EriArgs args, cons
     const int SA = dm.eb * dm.ec * dm.ed, SB = dm.ec * dm.ed, SC = dm.ed;   // table strides of a, b, c
     const int team = threadIdx.x / TQ, lane = threadIdx.x % TQ;
     double *s_rw = smem + (size_t)team * dm.team;   // nodes [0, NR), weights [NR, 2NR)
-    double *s_tab = s_rw + dm.rw;                   // [3][TSZ][NR]
+    double *s_G = s_rw + dm.rw;                     // [3][NR][gsz] 2-D recursion
+    double *s_tab = s_G + 3 * NR * dm.gsz;          // [3][TSZ][NR]
     double *s_gam = s_tab + 3 * NR * TSZ;           // [NCART]
     double *s_red = s_gam + NCART;                  // [9][TQ]
     const int n = args.n;
@@ -172,34 +177,39 @@ __global__ void __launch_bounds__(kBlk) eri_grad_kernel(const EriArgs args, cons
                     const double pa = dim == 0 ? pax : (dim == 1 ? pay : paz);
                     const double qc = dim == 0 ? qcx : (dim == 1 ? qcy : qcz);
                     const double pq = dim == 0 ? pqx : (dim == 1 ? pqy : pqz);
+                    grad_vrr(s_G + (size_t)(dim * NR + r) * dm.gsz, dm.l12, dm.l34, dim == 2 ? w * sr : 1.0, B00,
+                             B10, B01, pa - q * pq * f, qc + p * pq * f);
+                }
+            }
+            __syncthreads();
+            if (work) {
+                // transfer, one (direction, entry, root) per lane and step:
+                // I = sum_i C(b,i) ab^i sum_k C(d,k) cd^k G[a+b-i][c+d-k]
+                const int W = dm.l34 + 1;
+                const int njob = 3 * TSZ * NR;
+                for (int jb = lane; jb < njob; jb += TQ) {
+                    const int r = jb % NR, e = (jb / NR) % TSZ, dim = jb / (NR * TSZ);
+                    const int d = e % dm.ed, c = (e / dm.ed) % dm.ec, b = (e / SB) % dm.eb, a = e / SA;
+                    if (a + b > dm.l12 || c + d > dm.l34) continue;
                     const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
                     const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                    double G[8][8];
-                    grad_vrr(G, dm.l12, dm.l34, dim == 2 ? w * sr : 1.0, B00, B10, B01, pa - q * pq * f,
-                             qc + p * pq * f);
-                    double *tab = s_tab + (size_t)dim * TSZ * NR + r;
-                    for (int a = 0; a < dm.ea; ++a)
-                        for (int b = 0; b < dm.eb; ++b)
-                            for (int c = 0; c < dm.ec; ++c)
-                                for (int d = 0; d < dm.ed; ++d) {
-                                    if (a + b > dm.l12 || c + d > dm.l34) continue;
-                                    // I = sum_i C(b,i) ab^i sum_k C(d,k) cd^k G[a+b-i][c+d-k]
-                                    double s = 0.0, abp = 1.0;
-                                    int bi = 1;
-                                    for (int i = 0; i <= b; ++i) {
-                                        double t = 0.0, cdp = 1.0;
-                                        int bk = 1;
-                                        for (int k = 0; k <= d; ++k) {
-                                            t = fma(bk * cdp, G[a + b - i][c + d - k], t);
-                                            cdp *= cd;
-                                            bk = bk * (d - k) / (k + 1);
-                                        }
-                                        s = fma(bi * abp, t, s);
-                                        abp *= ab;
-                                        bi = bi * (b - i) / (i + 1);
-                                    }
-                                    tab[(size_t)(((a * dm.eb + b) * dm.ec + c) * dm.ed + d) * NR] = s;
-                                }
+                    const double *G = s_G + (size_t)(dim * NR + r) * dm.gsz;
+                    double sacc = 0.0, abp = 1.0;
+                    int bi = 1;
+                    for (int i = 0; i <= b; ++i) {
+                        const double *Gi = G + (a + b - i) * W + c + d;
+                        double t = 0.0, cdp = 1.0;
+                        int bk = 1;
+                        for (int k = 0; k <= d; ++k) {
+                            t = fma(bk * cdp, Gi[-k], t);
+                            cdp *= cd;
+                            bk = bk * (d - k) / (k + 1);
+                        }
+                        sacc = fma(bi * abp, t, sacc);
+                        abp *= ab;
+                        bi = bi * (b - i) / (i + 1);
+                    }
+                    s_tab[jb] = sacc;
                 }
             }
             __syncthreads();

@@ -113,6 +113,10 @@ struct ClassWork {
     int u0 = 0, nu = 0, v0 = 0, nv = 0, same = 0;   // bra and ket pair ranges
     long long total = 0;         // unscreened quartets of the class (all ranks)
     long long items = 0;         // work items of this rank: ceil((total - rank) / nranks)
+    // compacted lists: this class's survivors at [loff, loff + count) of the
+    // handle's list, the FP64 window (bound >= tau_mix, or all without mixed
+    // precision) first, nhi entries, then the FP32 window
+    long long loff = 0, nhi = 0;
 };
 
 static int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
@@ -144,6 +148,8 @@ struct patgpu_basis {
     // quartets
     std::vector<pg::ClassWork> work;
     long long nquart = 0, nquart_unscreened = 0;
+    pg::DBuf d_list;                 // compacted class quartet indices (uint64), when lists are on
+    bool lists = false;
     // work buffers
     pg::DBuf d_D0, d_D1, d_A0, d_A1, d_Pk0, d_Pk1, d_Gk0, d_Gk1, d_err;
     std::vector<double> h_stage;
@@ -365,10 +371,39 @@ static EriArgs class_args(const patgpu_basis *h, const ClassWork &w, int mode, d
 // With mixed precision on, the class runs twice over its pair space: the
 // tuned FP64 kernel on the quartets whose bound is at least tau_mix, the FP32
 // kernel on those between the screening threshold and tau_mix.
+// Arguments over the compacted list of class w: window 0 = the FP64 part
+// (everything without mixed precision), 1 = the FP32 part, 2 = all survivors.
+static EriArgs list_args(const patgpu_basis *h, const ClassWork &w, int mode, int window)
+{
+    EriArgs a = class_args(h, w, mode, -1.0, INFINITY);
+    const unsigned long long *l = h->d_list.as<unsigned long long>() + w.loff;
+    a.klist = window == 1 ? l + w.nhi : l;
+    a.nquart = window == 0 ? w.nhi : (window == 1 ? w.count - w.nhi : w.count);
+    return a;
+}
+
 static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const EriArgs &proto, cudaStream_t s)
 {
     const double lo = h->tau > 0.0 ? h->tau : -1.0;
     const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
+    if (h->lists) {
+        EriArgs a = list_args(h, w, proto.mode, 0);
+        a.D0 = proto.D0;
+        a.D1 = proto.D1;
+        a.A0 = proto.A0;
+        a.A1 = proto.A1;
+        if (a.nquart > 0) {
+            cudaError_t e = launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant);
+            if (e != cudaSuccess) return e;
+        }
+        if (!mixed) return cudaSuccess;
+        a = list_args(h, w, proto.mode, 1);
+        a.D0 = proto.D0;
+        a.D1 = proto.D1;
+        a.A0 = proto.A0;
+        a.A1 = proto.A1;
+        return a.nquart > 0 ? launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, 3) : cudaSuccess;
+    }
     EriArgs a = class_args(h, w, proto.mode, mixed ? h->tau_mix : lo, INFINITY);
     a.D0 = proto.D0;
     a.D1 = proto.D1;
@@ -391,6 +426,90 @@ __global__ void count_kernel(const EriArgs a, unsigned long long *cnt)
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, c);
+}
+
+// Stream compaction of one window of a class's implicit quartet space: the
+// class index k of every surviving item, appended at out[*cursor++] with
+// warp-aggregated atomics (order within a warp kept).
+__global__ void compact_kernel(const EriArgs a, unsigned long long *out, unsigned long long *cursor)
+{
+    for (long long qi0 = (long long)blockIdx.x * blockDim.x; qi0 < a.nquart;
+         qi0 += (long long)gridDim.x * blockDim.x) {
+        const long long qi = qi0 + threadIdx.x;
+        int u, v;
+        const bool keep = qi < a.nquart && eri_quartet_at(a, qi, u, v);
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (!m) continue;
+        const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+        unsigned long long base = 0;
+        if (lane == lead) base = atomicAdd(cursor, (unsigned long long)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (keep) out[base + __popc(m & ((1u << lane) - 1u))] = (unsigned long long)(qi * a.nranks + a.rank);
+    }
+}
+
+// Compacted quartet lists (8 bytes per surviving quartet), when they fit in
+// half of the free device memory and PATGPU_LISTS is not 0: the class
+// kernels then visit only surviving quartets instead of stepping their
+// teams through screened-out items.  With mixed precision on, each class's
+// list is split into its FP64 and FP32 windows.
+static int build_lists(patgpu_basis *h)
+{
+    h->lists = false;
+    const char *env = getenv("PATGPU_LISTS");
+    if (env && !strcmp(env, "0")) return 0;
+    long long total = 0;
+    for (auto &w : h->work) {
+        w.loff = total;
+        total += w.count;
+    }
+    size_t fr = 0, tot = 0;
+    PG_CUDA(cudaMemGetInfo(&fr, &tot));
+    const size_t bytes = sizeof(unsigned long long) * (size_t)std::max<long long>(total, 1);
+    if (bytes > h->d_list.bytes && bytes > fr / 2) return 0;
+    PG_CUDA(h->d_list.ensure(bytes));
+    const double lo = h->tau > 0.0 ? h->tau : -1.0;
+    const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
+    DBuf dcur;
+    const size_t nc = 2 * h->work.size();
+    PG_CUDA(dcur.ensure(sizeof(unsigned long long) * std::max<size_t>(nc, 1)));
+    PG_CUDA(cudaMemsetAsync(dcur.p, 0, sizeof(unsigned long long) * std::max<size_t>(nc, 1), h->stream));
+    unsigned long long *out = h->d_list.as<unsigned long long>();
+    for (size_t k = 0; k < h->work.size(); ++k) {
+        const ClassWork &w = h->work[k];
+        // FP64 window first, then the FP32 window behind it
+        EriArgs a = class_args(h, w, MODE_RHF, mixed ? h->tau_mix : lo, INFINITY);
+        const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
+        compact_kernel<<<std::max(g, 1), 256, 0, h->stream>>>(a, out + w.loff, dcur.as<unsigned long long>() + 2 * k);
+    }
+    PG_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> cur(std::max<size_t>(nc, 1), 0);
+    PG_CUDA(cudaMemcpyAsync(cur.data(), dcur.p, sizeof(unsigned long long) * cur.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+    PG_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t k = 0; k < h->work.size(); ++k) h->work[k].nhi = (long long)cur[2 * k];
+    if (mixed) {
+        for (size_t k = 0; k < h->work.size(); ++k) {
+            const ClassWork &w = h->work[k];
+            EriArgs a = class_args(h, w, MODE_RHF, lo, h->tau_mix);
+            const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
+            compact_kernel<<<std::max(g, 1), 256, 0, h->stream>>>(a, out + w.loff + w.nhi,
+                                                                  dcur.as<unsigned long long>() + 2 * k + 1);
+        }
+        PG_CUDA(cudaGetLastError());
+        PG_CUDA(cudaMemcpyAsync(cur.data(), dcur.p, sizeof(unsigned long long) * cur.size(), cudaMemcpyDeviceToHost,
+                                h->stream));
+        PG_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    for (size_t k = 0; k < h->work.size(); ++k) {
+        const ClassWork &w = h->work[k];
+        const long long got = (long long)cur[2 * k] + (mixed ? (long long)cur[2 * k + 1] : 0);
+        if (got != w.count)
+            return fail(PATGPU_ESTATE, "quartet list of class (%d%d|%d%d): %lld entries, %lld counted", w.la, w.lb,
+                        w.lc, w.ld, got, w.count);
+    }
+    h->lists = true;
+    return 0;
 }
 
 // Per class pair (bra class >= ket class): the pair ranges and the number of
@@ -438,16 +557,19 @@ static int build_quartets(patgpu_basis *h)
     }
     h->nquart = owned;
     h->nquart_unscreened = unscreened;
-    return 0;
+    return build_lists(h);
 }
 
 // Kernel-variant autotuner: every class has the lane team kernel (0) and the
 // shared-memory team kernel (2); the small classes also have the
-// register-only kernel (1).  Each variant is timed on the class's own
-// quartet list and the fastest kept.  Runs once per quartet list, on a zero
-// density and the handle's own accumulator (the results are discarded).
+// register-only kernel (1).  Each variant is timed on the first
+// kTuneItems work items of the class's own quartet space and the fastest
+// kept.  Runs once per quartet partition, on a zero density and the
+// handle's own accumulator (the results are discarded).
 // PATGPU_VARIANT=lane|reg|smem forces a choice where it exists.
 static int ensure_work(patgpu_basis *h, bool two);
+
+constexpr long long kTuneItems = 1 << 18;
 
 static int tune_variants(patgpu_basis *h)
 {
@@ -476,9 +598,10 @@ static int tune_variants(patgpu_basis *h)
     PG_CUDA(cudaEventCreate(&e0));
     PG_CUDA(cudaEventCreate(&e1));
     for (auto &w : h->work) {
-        a = class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
+        a = h->lists ? list_args(h, w, MODE_RHF, 0) : class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
         a.D0 = h->d_D0.as<double>();
         a.A0 = h->d_A0.as<double>();
+        a.nquart = std::min(a.nquart, kTuneItems);
         float best = 1e30f;
         for (int var = 0; var <= 2; ++var) {
             if (!eri_has_variant(w.la, w.lb, w.lc, w.ld, var)) continue;
@@ -651,7 +774,8 @@ static int grad_2e(patgpu_basis *h, const double *P, double *grad)
     ga.ea = h->d_pp_ea.as<double>();
     ga.grad = dg.as<double>();
     for (const auto &w : h->work) {
-        EriArgs a = class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
+        EriArgs a = h->lists ? list_args(h, w, MODE_RHF, 2)
+                             : class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
         a.D0 = h->d_D0.as<double>();
         ga.la = w.la;
         ga.lb = w.lb;
@@ -1012,7 +1136,7 @@ int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
     if (!h || !(tau_fp32 >= 0.0)) return fail(PATGPU_EINVAL, "bad mixed-precision threshold");
     h->tau_mix = tau_fp32;
     h->nquart_fp32 = 0;
-    if (tau_fp32 <= 0.0 || tau_fp32 <= h->tau) return 0;
+    if (tau_fp32 <= 0.0 || tau_fp32 <= h->tau) return h->lists ? build_lists(h) : 0;
     DBuf dcnt;
     PG_CUDA(dcnt.ensure(sizeof(unsigned long long)));
     PG_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long), h->stream));
@@ -1027,7 +1151,7 @@ int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
     PG_CUDA(cudaMemcpyAsync(&c, dcnt.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
     PG_CUDA(cudaStreamSynchronize(h->stream));
     h->nquart_fp32 = (long long)c;
-    return 0;
+    return h->lists ? build_lists(h) : 0;
 }
 
 int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32)

@@ -127,6 +127,43 @@ def test_scf_gradient_vs_energy_differences(dpm):
         assert abs(g[c, d] - fd) < 2e-6, (c, d, g[c, d], fd)
 
 
+def alkane_dpm(ncarbon: int) -> Basis:
+    """The alkane + DPM recipe at small size: s/p/d shells on every atom, a q=0
+    ghost at the centroid with s/p/d shells, DPM on with the positron at the
+    centroid.  The atom and ghost exponents are moderate (0.2*3^k) so that the
+    overlap stays well conditioned and the SCF energy converges to 1e-12 Eh;
+    the full-size recipe's 0.002*2.2^k ghost shells make S nearly singular."""
+    sym, xyz = configs.alkane(ncarbon, 0)
+    cen = xyz.mean(axis=0)
+    specs = []
+    for c in range(len(sym)):
+        heavy = sym[c] != "H"
+        for a in configs.even_tempered(0.2, 3.0, 4 if heavy else 3):
+            specs.append((0, c, [a], [1.0]))
+        for a in configs.even_tempered(0.3, 3.0, 2 if heavy else 1):
+            specs.append((1, c, [a], [1.0]))
+        if heavy:
+            specs.append((2, c, [0.8], [1.0]))
+    for l in (0, 1, 2):
+        for a in configs.even_tempered(0.2, 3.0, 2):
+            specs.append((l, len(sym), [a], [1.0]))
+    mol = configs.molecule_basis(sym, xyz, with_f=False)
+    q = np.concatenate([mol.charges, [0.0]])
+    return Basis.from_shell_list(q, np.vstack([xyz, cen[None, :]]), specs, nelec=mol.nelec, mult=1,
+                                 dpm=1).dpm_augmented(cen)
+
+
+def test_alkane_dpm_gradient_vs_energy_differences():
+    b = alkane_dpm(2)
+    res = scf.rhf(b, dpm=True)
+    assert res.converged
+    g = scf.rhf_gradient(b, res, dpm=True)
+    h = 1e-4
+    for c, d in [(0, 0), (2, 2), (b.skipcen, 0)]:
+        fd = (scf_energy(b.displaced(c, d, h), True) - scf_energy(b.displaced(c, d, -h), True)) / (2 * h)
+        assert abs(g[c, d] - fd) < 2e-6, (c, d, g[c, d], fd)
+
+
 def test_scf_gradient_invariances():
     b = configs.water_spd()
     res = scf.rhf(b)
