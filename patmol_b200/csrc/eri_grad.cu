@@ -16,6 +16,9 @@
 // classes instead of 55 instantiations.
 #include "eri_grad.cuh"
 
+#include <mutex>
+#include <vector>
+
 namespace pg {
 
 extern __constant__ RysConst c_rys;
@@ -30,9 +33,86 @@ constexpr int kBlk = 128;
 
 struct GradDims {
     int la, lb, lc, ld, na, nb, nc, nd, ncart;
-    int nr, l12, l34, ea, eb, ec, ed, tsz, gsz;
+    int nr, nrp, l12, l34, ea, eb, ec, ed, tsz, gsz, nvalid;
     int tq, nteam, rw, team;   // team: doubles of shared memory per team
+    const int4 *desc;          // per component: table entries, exponents, component indices
+    const int2 *ent;           // per valid transfer entry: table index, (a, b, c, d)
 };
+
+// Host-built index tables of every class (uploaded once per process):
+//  desc[c] = {e_x | e_y << 10 | e_z << 20,   1-D table entry of component c per direction
+//             exponents (a, b, c of the quartet) per direction, 2 bits each,
+//             ia | ib << 4 | ic << 8 | id << 12,   component indices
+//             0}
+//  ent[k]  = {table index e, a | b << 4 | c << 8 | d << 12} for the entries
+//             with a + b <= la + lb + 1 and c + d <= lc + ld + 1.
+struct GradTables {
+    int4 *desc = nullptr;
+    int2 *ent = nullptr;
+    long long doff[4][4][4][4], eoff[4][4][4][4];
+    int nvalid[4][4][4][4];
+    cudaError_t status = cudaSuccess;
+};
+
+int cexp_host(int l, int k, int dir)
+{
+    int n = 0;
+    for (int lx = l; lx >= 0; --lx)
+        for (int ly = l - lx; ly >= 0; --ly) {
+            if (n == k) return dir == 0 ? lx : (dir == 1 ? ly : l - lx - ly);
+            ++n;
+        }
+    return 0;
+}
+
+const GradTables &grad_tables()
+{
+    static GradTables t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        std::vector<int4> desc;
+        std::vector<int2> ent;
+        auto nc = [](int l) { return (l + 1) * (l + 2) / 2; };
+        for (int la = 0; la < 4; ++la)
+            for (int lb = 0; lb <= la; ++lb)
+                for (int lc = 0; lc < 4; ++lc)
+                    for (int ld = 0; ld <= lc; ++ld) {
+                        const int EB = lb + 2, EC = lc + 2, ED = ld + 1;
+                        t.doff[la][lb][lc][ld] = (long long)desc.size();
+                        for (int ia = 0; ia < nc(la); ++ia)
+                            for (int ib = 0; ib < nc(lb); ++ib)
+                                for (int ic = 0; ic < nc(lc); ++ic)
+                                    for (int id = 0; id < nc(ld); ++id) {
+                                        int e = 0, x = 0;
+                                        for (int dim = 0; dim < 3; ++dim) {
+                                            const int a = cexp_host(la, ia, dim), b = cexp_host(lb, ib, dim);
+                                            const int c = cexp_host(lc, ic, dim), d = cexp_host(ld, id, dim);
+                                            e |= (((a * EB + b) * EC + c) * ED + d) << (10 * dim);
+                                            x |= (a | b << 2 | c << 4) << (6 * dim);
+                                        }
+                                        desc.push_back(make_int4(e, x, ia | ib << 4 | ic << 8 | id << 12, 0));
+                                    }
+                        t.eoff[la][lb][lc][ld] = (long long)ent.size();
+                        int nv = 0;
+                        for (int a = 0; a < la + 2; ++a)
+                            for (int b = 0; b < EB; ++b)
+                                for (int c = 0; c < EC; ++c)
+                                    for (int d = 0; d < ED; ++d) {
+                                        if (a + b > la + lb + 1 || c + d > lc + ld + 1) continue;
+                                        ent.push_back(make_int2(((a * EB + b) * EC + c) * ED + d,
+                                                                a | b << 4 | c << 8 | d << 12));
+                                        ++nv;
+                                    }
+                        t.nvalid[la][lb][lc][ld] = nv;
+                    }
+        cudaError_t e = cudaMalloc(&t.desc, sizeof(int4) * desc.size());
+        if (e == cudaSuccess) e = cudaMalloc(&t.ent, sizeof(int2) * ent.size());
+        if (e == cudaSuccess) e = cudaMemcpy(t.desc, desc.data(), sizeof(int4) * desc.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(t.ent, ent.data(), sizeof(int2) * ent.size(), cudaMemcpyHostToDevice);
+        t.status = e;
+    });
+    return t;
+}
 
 // Lanes per team: the transfer and contraction phases spread over all of
 // them, so mid-size classes take whole warps and large ones a block.
@@ -56,10 +136,11 @@ GradDims grad_dims(int la, int lb, int lc, int ld)
     d.ea = la + 2; d.eb = lb + 2; d.ec = lc + 2; d.ed = ld + 1;
     d.tsz = d.ea * d.eb * d.ec * d.ed;
     d.gsz = (d.l12 + 1) * (d.l34 + 1);
+    d.nrp = d.nr | 1;   // odd root stride: lanes reading neighbouring entries hit different banks
     d.tq = tq_for(d.ncart);
     d.nteam = kBlk / d.tq;
     d.rw = (2 * d.nr + 1) / 2 * 2;
-    d.team = (d.rw + 3 * d.nr * d.gsz + 3 * d.nr * d.tsz + d.ncart + 9 * d.tq + 1) / 2 * 2;
+    d.team = (d.rw + 3 * d.nr * d.gsz + 3 * d.nrp * d.tsz + d.ncart + 9 * d.tq + 1) / 2 * 2;
     return d;
 }
 
@@ -86,14 +167,14 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
     __shared__ int s_np[kBlk / 8];
     __shared__ int s_maxp;
 
-    const int TQ = dm.tq, NTEAM = dm.nteam, NR = dm.nr, TSZ = dm.tsz;
-    const int NB = dm.nb, NC = dm.nc, ND = dm.nd, NCART = dm.ncart;
+    const int TQ = dm.tq, NTEAM = dm.nteam, NR = dm.nr, NRP = dm.nrp, TSZ = dm.tsz;
+    const int NCART = dm.ncart;
     const int SA = dm.eb * dm.ec * dm.ed, SB = dm.ec * dm.ed, SC = dm.ed;   // table strides of a, b, c
     const int team = threadIdx.x / TQ, lane = threadIdx.x % TQ;
     double *s_rw = smem + (size_t)team * dm.team;   // nodes [0, NR), weights [NR, 2NR)
     double *s_G = s_rw + dm.rw;                     // [3][NR][gsz] 2-D recursion
-    double *s_tab = s_G + 3 * NR * dm.gsz;          // [3][TSZ][NR]
-    double *s_gam = s_tab + 3 * NR * TSZ;           // [NCART]
+    double *s_tab = s_G + 3 * NR * dm.gsz;          // [3][TSZ][NRP]
+    double *s_gam = s_tab + 3 * NRP * TSZ;          // [NCART]
     double *s_red = s_gam + NCART;                  // [9][TQ]
     const int n = args.n;
     const double *__restrict__ P = args.D0;
@@ -118,7 +199,8 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
             const bool sab = args.pr.sa[u] == args.pr.sb[u], scd = args.pr.sa[v] == args.pr.sb[v];
             const double deg = (sab ? 1.0 : 2.0) * (scd ? 1.0 : 2.0) * (u == v ? 1.0 : 2.0);
             for (int c = lane; c < NCART; c += TQ) {
-                const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
+                const int ci = __ldg(&dm.desc[c].z);
+                const int ia = ci & 15, ib = (ci >> 4) & 15, ic = (ci >> 8) & 15, id = ci >> 12;
                 const int i = fa + ia, j = fb + ib, k = fc + ic, l = fd + id;
                 const double g = 2.0 * __ldg(P + (size_t)i * n + j) * __ldg(P + (size_t)k * n + l) -
                                  0.5 * (__ldg(P + (size_t)i * n + k) * __ldg(P + (size_t)j * n + l) +
@@ -183,63 +265,62 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
             }
             __syncthreads();
             if (work) {
-                // transfer, one (direction, entry, root) per lane and step:
+                // transfer, one (direction, valid entry) per lane and step, all roots:
                 // I = sum_i C(b,i) ab^i sum_k C(d,k) cd^k G[a+b-i][c+d-k]
-                const int W = dm.l34 + 1;
-                const int njob = 3 * TSZ * NR;
-                for (int jb = lane; jb < njob; jb += TQ) {
-                    const int r = jb % NR, e = (jb / NR) % TSZ, dim = jb / (NR * TSZ);
-                    const int d = e % dm.ed, c = (e / dm.ed) % dm.ec, b = (e / SB) % dm.eb, a = e / SA;
-                    if (a + b > dm.l12 || c + d > dm.l34) continue;
+                const int W = dm.l34 + 1, NV = dm.nvalid;
+                for (int jb = lane; jb < 3 * NV; jb += TQ) {
+                    const int dim = jb >= 2 * NV ? 2 : (jb >= NV ? 1 : 0), k0 = jb - dim * NV;
+                    const int2 en = __ldg(&dm.ent[k0]);
+                    const int a = en.y & 15, b = (en.y >> 4) & 15, c = (en.y >> 8) & 15, d = en.y >> 12;
                     const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
                     const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                    const double *G = s_G + (size_t)(dim * NR + r) * dm.gsz;
-                    double sacc = 0.0, abp = 1.0;
-                    int bi = 1;
-                    for (int i = 0; i <= b; ++i) {
-                        const double *Gi = G + (a + b - i) * W + c + d;
-                        double t = 0.0, cdp = 1.0;
-                        int bk = 1;
-                        for (int k = 0; k <= d; ++k) {
-                            t = fma(bk * cdp, Gi[-k], t);
-                            cdp *= cd;
-                            bk = bk * (d - k) / (k + 1);
+                    double cb[5], cdk[4];   // C(b,i) ab^i and C(d,k) cd^k (b <= 4, d <= 3)
+                    cb[0] = 1.0;
+                    cdk[0] = 1.0;
+#pragma unroll
+                    for (int i = 1; i < 5; ++i) cb[i] = i <= b ? cb[i - 1] * ab * (double)(b - i + 1) / (double)i : 0.0;
+#pragma unroll
+                    for (int k = 1; k < 4; ++k) cdk[k] = k <= d ? cdk[k - 1] * cd * (double)(d - k + 1) / (double)k : 0.0;
+                    const double *G = s_G + (size_t)dim * NR * dm.gsz + (a + b) * W + c + d;
+                    double *out = s_tab + ((size_t)dim * TSZ + en.x) * NRP;
+                    for (int r = 0; r < NR; ++r) {
+                        const double *Gr = G + r * dm.gsz;
+                        double sacc = 0.0;
+#pragma unroll
+                        for (int i = 0; i < 5; ++i) {
+                            if (i > b) break;
+                            double t = 0.0;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                if (k > d) break;
+                                t = fma(cdk[k], Gr[-i * W - k], t);
+                            }
+                            sacc = fma(cb[i], t, sacc);
                         }
-                        sacc = fma(bi * abp, t, sacc);
-                        abp *= ab;
-                        bi = bi * (b - i) / (i + 1);
+                        out[r] = sacc;
                     }
-                    s_tab[jb] = sacc;
                 }
             }
             __syncthreads();
             if (work) {
                 const double ta = 2.0 * alpha, tb = 2.0 * beta, tc = 2.0 * gamma;
                 for (int c = lane; c < NCART; c += TQ) {
-                    const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
-                    const int ea = c_cart[dm.la][ia], eb = c_cart[dm.lb][ib], ec = c_cart[dm.lc][ic],
-                              ed = c_cart[dm.ld][id];
-                    int e0[3];
-#pragma unroll
-                    for (int dim = 0; dim < 3; ++dim) {
-                        const int sh = 4 * dim;
-                        e0[dim] = (((ea >> sh) & 15) * dm.eb + ((eb >> sh) & 15)) * dm.ec * dm.ed +
-                                  ((ec >> sh) & 15) * dm.ed + ((ed >> sh) & 15);
-                    }
+                    const int4 ds = __ldg(&dm.desc[c]);
+                    const int e0[3] = {ds.x & 1023, (ds.x >> 10) & 1023, ds.x >> 20};
                     const double gm = s_gam[c];
 #pragma unroll
                     for (int dim = 0; dim < 3; ++dim) {
-                        const int sh = 4 * dim;
-                        const int xa = (ea >> sh) & 15, xb = (eb >> sh) & 15, xc = (ec >> sh) & 15;
+                        const int xs = ds.y >> (6 * dim);
+                        const int xa = xs & 3, xb = (xs >> 2) & 3, xc = (xs >> 4) & 3;
                         const int d1 = dim == 0 ? 1 : 0, d2 = dim == 2 ? 1 : 2;
-                        const double *t0 = s_tab + (size_t)dim * TSZ * NR;
-                        const double *t1 = s_tab + ((size_t)d1 * TSZ + e0[d1]) * NR;
-                        const double *t2 = s_tab + ((size_t)d2 * TSZ + e0[d2]) * NR;
+                        const double *t0 = s_tab + (size_t)dim * TSZ * NRP;
+                        const double *t1 = s_tab + ((size_t)d1 * TSZ + e0[d1]) * NRP;
+                        const double *t2 = s_tab + ((size_t)d2 * TSZ + e0[d2]) * NRP;
                         // lowered entries are read only when the exponent is positive
                         const int e = e0[dim];
-                        const double *pa1 = t0 + (size_t)(e + SA) * NR, *ma1 = t0 + (size_t)(xa > 0 ? e - SA : e) * NR;
-                        const double *pb1 = t0 + (size_t)(e + SB) * NR, *mb1 = t0 + (size_t)(xb > 0 ? e - SB : e) * NR;
-                        const double *pc1 = t0 + (size_t)(e + SC) * NR, *mc1 = t0 + (size_t)(xc > 0 ? e - SC : e) * NR;
+                        const double *pa1 = t0 + (size_t)(e + SA) * NRP, *ma1 = t0 + (size_t)(xa > 0 ? e - SA : e) * NRP;
+                        const double *pb1 = t0 + (size_t)(e + SB) * NRP, *mb1 = t0 + (size_t)(xb > 0 ? e - SB : e) * NRP;
+                        const double *pc1 = t0 + (size_t)(e + SC) * NRP, *mc1 = t0 + (size_t)(xc > 0 ? e - SC : e) * NRP;
                         double sA = 0.0, sB = 0.0, sC = 0.0;
                         for (int r = 0; r < NR; ++r) {
                             const double o = t1[r] * t2[r];
@@ -295,7 +376,12 @@ cudaError_t launch_eri_grad(const EriArgs &a, const GradArgs &g, cudaStream_t st
 {
     if (g.la < 0 || g.la > 3 || g.lb < 0 || g.lb > g.la || g.lc < 0 || g.lc > 3 || g.ld < 0 || g.ld > g.lc)
         return cudaErrorInvalidValue;
-    const GradDims d = grad_dims(g.la, g.lb, g.lc, g.ld);
+    GradDims d = grad_dims(g.la, g.lb, g.lc, g.ld);
+    const GradTables &t = grad_tables();
+    if (t.status != cudaSuccess) return t.status;
+    d.desc = t.desc + t.doff[g.la][g.lb][g.lc][g.ld];
+    d.ent = t.ent + t.eoff[g.la][g.lb][g.lc][g.ld];
+    d.nvalid = t.nvalid[g.la][g.lb][g.lc][g.ld];
     const size_t smem = sizeof(double) * (size_t)d.team * d.nteam;
     static size_t configured = 0;
     if (smem > configured) {
