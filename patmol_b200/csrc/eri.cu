@@ -30,7 +30,8 @@ cudaError_t upload_rys_constants(const RysConst &rc)
 
 #define PG_KERNEL(la, lb, lc, ld, sw)                                                              \
     extern template cudaError_t launch_one<la, lb, lc, ld, 1>(const EriArgs &, cudaStream_t, int); \
-    extern template cudaError_t launch_one<la, lb, lc, ld, 2>(const EriArgs &, cudaStream_t, int);
+    extern template cudaError_t launch_one<la, lb, lc, ld, 2>(const EriArgs &, cudaStream_t, int); \
+    extern template cudaError_t launch_one<la, lb, lc, ld, 1, float>(const EriArgs &, cudaStream_t, int);
 #include "eri_kernels.inc"
 #undef PG_KERNEL
 
@@ -41,6 +42,7 @@ cudaError_t upload_rys_constants(const RysConst &rc)
         (sw == 1 && LA == lc && LB == ld && LC == la && LD == lb)) {                        \
         EriArgs b = a;                                                                       \
         b.swap = sw;                                                                         \
+        if (variant == 4) return launch_one<la, lb, lc, ld, 1, float>(b, stream, num_sms);  \
         return a.mode == MODE_UHF ? launch_one<la, lb, lc, ld, 2>(b, stream, num_sms)       \
                                   : launch_one<la, lb, lc, ld, 1>(b, stream, num_sms);      \
     }
@@ -59,7 +61,7 @@ cudaError_t upload_rys_constants(const RysConst &rc)
 
 bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 {
-    if (variant == 0 || variant == 2 || variant == 3) return true;
+    if (variant == 0 || variant == 2 || variant == 3 || variant == 4) return true;
 #define PG_REG(la, lb, lc, ld) \
     if (LA == la && LB == lb && LC == lc && LD == ld) return variant == 1;
 #include "eri_reg_classes.inc"
@@ -70,6 +72,7 @@ bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 cudaError_t launch_eri_class(int LA, int LB, int LC, int LD, const EriArgs &a, cudaStream_t stream,
                              int num_sms, int variant)
 {
+    if (variant == 4 && a.mode == MODE_UHF) variant = 3;   // the FP32 lane kernel has one density set
     if (variant == 2 || variant == 3) {
 #define PG_CLASS(la, lb, lc, ld)                                                     \
     if (LA == la && LB == lb && LC == lc && LD == ld) {                             \

@@ -63,7 +63,8 @@ struct EriArgs {
 // variant 0: the lane-per-ket-component team kernel (eri_kernel.cuh, every
 // class); 1: the register-only kernel (eri_reg.cuh, the classes of
 // eri_reg_classes.inc); 2: the shared-memory team kernel (eri_smem.cuh,
-// every class).
+// every class); 3 and 4: the FP32 forms of 2 and 0 (mixed precision; 4
+// takes one density set and runs as 3 for UHF).
 cudaError_t launch_eri_class(int la, int lb, int lc, int ld, const EriArgs &a, cudaStream_t stream,
                              int num_sms, int variant = 0);
 bool eri_has_variant(int la, int lb, int lc, int ld, int variant);

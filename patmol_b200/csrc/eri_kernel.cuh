@@ -103,12 +103,11 @@ struct Shape {
 
 // 2-D recursion and binomial transfer for one root and one direction;
 // writes I[a][b][c][d] to tab[(c(LD+1)+d) * TAB + a(LB+1)+b].
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void vrr_hrr(double *__restrict__ tab, double g00, double B00, double B10,
-                                        double B01, double C, double Cp, double ab, double cd)
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void vrr_hrr(R *__restrict__ tab, R g00, R B00, R B10, R B01, R C, R Cp, R ab, R cd)
 {
     constexpr int L12 = LA + LB, L34 = LC + LD, TAB = (LA + 1) * (LB + 1);
-    double G[L12 + 1][L34 + 1];
+    R G[L12 + 1][L34 + 1];
     G[0][0] = g00;
     if (L12 > 0) G[1][0] = C * g00;
 #pragma unroll
@@ -117,17 +116,17 @@ __device__ __forceinline__ void vrr_hrr(double *__restrict__ tab, double g00, do
     for (int j = 0; j < L34; ++j) {
 #pragma unroll
         for (int i = 0; i <= L12; ++i) {
-            double v = Cp * G[i][j];
-            if (j > 0) v = fma(j * B01, G[i][j - 1], v);
-            if (i > 0) v = fma(i * B00, G[i - 1][j], v);
+            R v = Cp * G[i][j];
+            if (j > 0) v = fma(R(j) * B01, G[i][j - 1], v);
+            if (i > 0) v = fma(R(i) * B00, G[i - 1][j], v);
             G[i][j + 1] = v;
         }
     }
-    double cdp[LD + 1], abp[LB + 1];
-    cdp[0] = 1.0;
+    R cdp[LD + 1], abp[LB + 1];
+    cdp[0] = R(1);
 #pragma unroll
     for (int k = 1; k <= LD; ++k) cdp[k] = cdp[k - 1] * cd;
-    abp[0] = 1.0;
+    abp[0] = R(1);
 #pragma unroll
     for (int k = 1; k <= LB; ++k) abp[k] = abp[k - 1] * ab;
 #pragma unroll
@@ -135,21 +134,21 @@ __device__ __forceinline__ void vrr_hrr(double *__restrict__ tab, double g00, do
 #pragma unroll
         for (int d = 0; d <= LD; ++d) {
             // ket transfer for every bra index: H[i] = sum_k C(d,k) cd^k G[i][c+d-k]
-            double H[L12 + 1];
+            R H[L12 + 1];
 #pragma unroll
             for (int i = 0; i <= L12; ++i) {
-                double t = 0.0;
+                R t = R(0);
 #pragma unroll
-                for (int k = 0; k <= d; ++k) t = fma(binom(d, k) * cdp[k], G[i][c + d - k], t);
+                for (int k = 0; k <= d; ++k) t = fma(R(binom(d, k)) * cdp[k], G[i][c + d - k], t);
                 H[i] = t;
             }
 #pragma unroll
             for (int a = 0; a <= LA; ++a)
 #pragma unroll
                 for (int b = 0; b <= LB; ++b) {
-                    double s = 0.0;
+                    R s = R(0);
 #pragma unroll
-                    for (int i = 0; i <= b; ++i) s = fma(binom(b, i) * abp[i], H[a + b - i], s);
+                    for (int i = 0; i <= b; ++i) s = fma(R(binom(b, i)) * abp[i], H[a + b - i], s);
                     tab[(c * (LD + 1) + d) * TAB + a * (LB + 1) + b] = s;
                 }
         }
@@ -157,9 +156,9 @@ __device__ __forceinline__ void vrr_hrr(double *__restrict__ tab, double g00, do
 
 // acc[j] += sum_r X Y Z for bra components CH0 .. CH0+CHN-1 (compile time);
 // X, Y, Z point at this lane's slices of root 0, RSTRIDE doubles per root.
-template <int LA, int LB, int NR, int RSTRIDE, int CH0, int CHN>
-__device__ __forceinline__ void assemble(double (&acc)[CHN], const double *__restrict__ X,
-                                         const double *__restrict__ Y, const double *__restrict__ Z)
+template <int LA, int LB, int NR, int RSTRIDE, int CH0, int CHN, typename R>
+__device__ __forceinline__ void assemble(R (&acc)[CHN], const R *__restrict__ X, const R *__restrict__ Y,
+                                         const R *__restrict__ Z)
 {
     constexpr int NB = ncart(LB), NAB = ncart(LA) * ncart(LB);
 #pragma unroll
@@ -178,7 +177,10 @@ __device__ __forceinline__ void assemble(double (&acc)[CHN], const double *__res
     }
 }
 
-template <int LA, int LB, int LC, int LD, int NDEN>
+// R: arithmetic type of the recursion, tables and integrals (float: the
+// mixed-precision form -- roots, weights, prefactors and every digestion
+// product and J/K sum stay FP64).
+template <int LA, int LB, int LC, int LD, int NDEN, typename R = double>
 __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, NDEN>::BLK, Shape<LA, LB, LC, LD, NDEN>::MINB)
 eri_class_kernel(const EriArgs args)
 {
@@ -261,11 +263,11 @@ eri_class_kernel(const EriArgs args)
         const int maxp = s_maxp;
 
         // integrals of every bra component for this lane's ket component
-        double acc[NCH][CH];
+        R acc[NCH][CH];
 #pragma unroll
         for (int c = 0; c < NCH; ++c)
 #pragma unroll
-            for (int j = 0; j < CH; ++j) acc[c][j] = 0.0;
+            for (int j = 0; j < CH; ++j) acc[c][j] = R(0);
 
         for (int ip = 0; ip < maxp; ++ip) {
             bool work = active && ip < npb * npk;
@@ -304,15 +306,17 @@ eri_class_kernel(const EriArgs args)
                     const double pq = dim == 0 ? pqx : (dim == 1 ? pqy : pqz);
                     const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
                     const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                    vrr_hrr<LA, LB, LC, LD>(s_tab + (dim * NR + r) * TSZ, dim == 2 ? w * sr : 1.0, B00, B10, B01,
-                                            pa - q * pq * f, qc + p * pq * f, ab, cd);
+                    vrr_hrr<LA, LB, LC, LD, R>(reinterpret_cast<R *>(s_tab) + (dim * NR + r) * TSZ,
+                                               R(dim == 2 ? w * sr : 1.0), R(B00), R(B10), R(B01),
+                                               R(pa - q * pq * f), R(qc + p * pq * f), R(ab), R(cd));
                 }
             }
             __syncthreads();
             if (work) {
-                const double *X = s_tab + tcdx * TAB;
-                const double *Y = s_tab + NR * TSZ + tcdy * TAB;
-                const double *Z = s_tab + 2 * NR * TSZ + tcdz * TAB;
+                const R *tb = reinterpret_cast<const R *>(s_tab);
+                const R *X = tb + tcdx * TAB;
+                const R *Y = tb + NR * TSZ + tcdy * TAB;
+                const R *Z = tb + 2 * NR * TSZ + tcdz * TAB;
                 assemble<LA, LB, NR, TSZ, 0, CH>(acc[0], X, Y, Z);
                 if constexpr (NCH > 1) assemble<LA, LB, NR, TSZ, CH, CH>(acc[1], X, Y, Z);
                 if constexpr (NCH > 2) assemble<LA, LB, NR, TSZ, 2 * CH, CH>(acc[2], X, Y, Z);
@@ -334,7 +338,7 @@ eri_class_kernel(const EriArgs args)
                         if (ab < NAB) {
                             // the caller's orientation: (quart.x pair | quart.y pair)
                             const size_t oi = args.swap ? (size_t)lane * NAB + ab : (size_t)ab * NCD + lane;
-                            o[oi] = acc[c][j] * nfk * c_norm[LA][ab / NB] * c_norm[LB][ab % NB];
+                            o[oi] = (double)acc[c][j] * nfk * c_norm[LA][ab / NB] * c_norm[LB][ab % NB];
                         }
                     }
             }
@@ -369,7 +373,7 @@ eri_class_kernel(const EriArgs args)
                     const int ab = c * CH + j;
                     if (ab < NAB) {
                         const int ia = ab / NB, ib = ab % NB;
-                        const double I = acc[c][j];
+                        const double I = (double)acc[c][j];
                         double dab = s_db[ab];
                         if (NDEN == 2) dab += s_db[NDB + ab];
                         jcd = fma(I, dab, jcd);
@@ -400,7 +404,7 @@ eri_class_kernel(const EriArgs args)
                         const int ab = c * CH + j;
                         if (ab < NAB) {
                             const int ia = ab / NB, ib = ab % NB;
-                            const double o = sJ * acc[c][j] * Dcd * c_norm[LA][ia] * c_norm[LB][ib];
+                            const double o = sJ * (double)acc[c][j] * Dcd * c_norm[LA][ia] * c_norm[LB][ib];
                             const size_t idx = (size_t)(fa + ia) * n + fb + ib;
                             atomicAdd(args.A0 + idx, o);
                             if (NDEN == 2) atomicAdd(args.A1 + idx, o);
@@ -484,13 +488,13 @@ eri_class_kernel(const EriArgs args)
     }
 }
 
-template <int LA, int LB, int LC, int LD, int NDEN>
+template <int LA, int LB, int LC, int LD, int NDEN, typename R = double>
 cudaError_t launch_one(const EriArgs &a, cudaStream_t stream, int num_sms)
 {
     using S = Shape<LA, LB, LC, LD, NDEN>;
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(eri_class_kernel<LA, LB, LC, LD, NDEN>,
+        cudaError_t e = cudaFuncSetAttribute(eri_class_kernel<LA, LB, LC, LD, NDEN, R>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
         configured = true;
@@ -499,7 +503,7 @@ cudaError_t launch_one(const EriArgs &a, cudaStream_t stream, int num_sms)
     long long cap = (long long)num_sms * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
-    eri_class_kernel<LA, LB, LC, LD, NDEN><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
+    eri_class_kernel<LA, LB, LC, LD, NDEN, R><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
     return cudaGetLastError();
 }
 

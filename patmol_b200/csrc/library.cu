@@ -110,6 +110,7 @@ struct ClassWork {
     int la, lb, lc, ld;
     long long offset, count;     // count: quartets this rank owns after screening
     int variant = 0;             // kernel variant chosen for this class (see tune_variants)
+    int variant32 = 3;           // FP32 kernel of the mixed-precision window (3 or 4, see tune_fp32)
     int u0 = 0, nu = 0, v0 = 0, nv = 0, same = 0;   // bra and ket pair ranges
     long long total = 0;         // unscreened quartets of the class (all ranks)
     long long items = 0;         // work items of this rank: ceil((total - rank) / nranks)
@@ -402,7 +403,8 @@ static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const 
         a.D1 = proto.D1;
         a.A0 = proto.A0;
         a.A1 = proto.A1;
-        return a.nquart > 0 ? launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, 3) : cudaSuccess;
+        return a.nquart > 0 ? launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant32)
+                            : cudaSuccess;
     }
     EriArgs a = class_args(h, w, proto.mode, mixed ? h->tau_mix : lo, INFINITY);
     a.D0 = proto.D0;
@@ -413,7 +415,7 @@ static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const 
     if (e != cudaSuccess || !mixed) return e;
     a.tau_lo = lo;
     a.tau_hi = h->tau_mix;
-    return launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, 3);
+    return launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant32);
 }
 
 __global__ void count_kernel(const EriArgs a, unsigned long long *cnt)
@@ -616,6 +618,56 @@ static int tune_variants(patgpu_basis *h)
             if (ms < best) {
                 best = ms;
                 w.variant = var;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
+// FP32 variant per class for the mixed-precision window: the shared-memory
+// kernel (3) against the lane kernel (4), timed like tune_variants on the
+// first kTuneItems quartets of the window.  PATGPU_VARIANT32=smem|lane
+// forces one.
+static int tune_fp32(patgpu_basis *h)
+{
+    const char *force = getenv("PATGPU_VARIANT32");
+    for (auto &w : h->work) w.variant32 = 3;
+    if (force && !strcmp(force, "smem")) return 0;
+    if (force && !strcmp(force, "lane")) {
+        for (auto &w : h->work) w.variant32 = 4;
+        return 0;
+    }
+    if (h->work.empty() || h->tau_mix <= 0.0) return 0;
+    int rc = ensure_work(h, false);
+    if (rc) return rc;
+    const size_t nn = (size_t)h->n * h->n;
+    cudaStream_t s = h->stream;
+    PG_CUDA(cudaMemsetAsync(h->d_D0.p, 0, sizeof(double) * nn, s));
+    cudaEvent_t e0, e1;
+    PG_CUDA(cudaEventCreate(&e0));
+    PG_CUDA(cudaEventCreate(&e1));
+    const double lo = h->tau > 0.0 ? h->tau : -1.0;
+    for (auto &w : h->work) {
+        EriArgs a = h->lists ? list_args(h, w, MODE_RHF, 1) : class_args(h, w, MODE_RHF, lo, h->tau_mix);
+        if (a.nquart <= 0) continue;
+        a.D0 = h->d_D0.as<double>();
+        a.A0 = h->d_A0.as<double>();
+        a.nquart = std::min(a.nquart, kTuneItems);
+        float best = 1e30f;
+        for (int var = 3; var <= 4; ++var) {
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {
+                PG_CUDA(cudaEventRecord(e0, s));
+                PG_CUDA(launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, var));
+                PG_CUDA(cudaEventRecord(e1, s));
+                PG_CUDA(cudaEventSynchronize(e1));
+                PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            }
+            if (ms < best) {
+                best = ms;
+                w.variant32 = var;
             }
         }
     }
@@ -1151,7 +1203,8 @@ int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
     PG_CUDA(cudaMemcpyAsync(&c, dcnt.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
     PG_CUDA(cudaStreamSynchronize(h->stream));
     h->nquart_fp32 = (long long)c;
-    return h->lists ? build_lists(h) : 0;
+    int rc = h->lists ? build_lists(h) : 0;
+    return rc ? rc : tune_fp32(h);
 }
 
 int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32)

@@ -51,3 +51,13 @@ def test_mixed_organic_molecule():
     nfp32, nq, dg, de = mixed_vs_fp64(b)
     assert nfp32 > 0.05 * nq
     assert dg < 1e-7 and abs(de) < 1e-6, (nfp32, nq, dg, de)
+
+
+@pytest.mark.parametrize("variant32", ["smem", "lane"])
+def test_mixed_each_fp32_kernel(variant32, monkeypatch):
+    """Both FP32 kernels (shared-memory and lane), forced for every class."""
+    monkeypatch.setenv("PATGPU_VARIANT32", variant32)
+    b = configs.organic_basis(6, seed=4)
+    nfp32, nq, dg, de = mixed_vs_fp64(b)
+    assert nfp32 > 0.05 * nq
+    assert dg < 1e-7 and abs(de) < 1e-6, (variant32, nfp32, nq, dg, de)
