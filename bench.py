@@ -40,9 +40,10 @@ WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 function
 # workload, from one ncu capture of dram__bytes_read.sum and
 # dram__bytes_write.sum (cold caches per launch); the capture's command and
 # per-kernel figures are kept with the other ncu summaries under profiles/.
-STEP_DRAM_BYTES = 163.7e6
+STEP_DRAM_BYTES = 219.1e6
 STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 55 class kernels of one "
-                    "Fock build (37.9 MB read, 125.8 MB write, mostly local-memory write-back of three f classes)")
+                    "Fock build (91.2 MB read incl. 58 MB of compacted quartet lists, 127.9 MB write, mostly "
+                    "local-memory write-back of three f classes)")
 
 
 def parse():
@@ -57,15 +58,17 @@ def parse():
                     help="Schwarz bound below which the mixed-precision leg runs quartets in FP32")
     ap.add_argument("--batch-molecules", type=int, default=32,
                     help="molecules in the batched (lock-step, graph-captured) leg; 0 skips it")
+    ap.add_argument("--batch-max-atoms", type=int, default=8,
+                    help="molecule sizes of the batched leg are uniform in 3..this")
     ap.add_argument("--alkane-carbons", type=int, default=12)
     ap.add_argument("--scf-iters", type=int, default=3,
                     help="alkane_dpm: SCF iterations before the gradient (timing; the converged "
                          "finite-difference check runs at C3H8 size in the GPU tests)")
     ap.add_argument("--workload", default="water_positron",
-                    choices=["water_positron", "organic40", "alkane_dpm"],
+                    choices=["water_positron", "organic40", "alkane_dpm", "batch"],
                     help="water_positron: the headline line; organic40: FP64 vs mixed Fock build of the "
                          "40-atom organic molecule; alkane_dpm: SCF and analytic gradient of C12H26 with "
-                         "positron shells and DPM (one GPU)")
+                         "positron shells and DPM (one GPU); batch: the batched leg alone")
     return ap.parse_args()
 
 
@@ -175,7 +178,7 @@ def batched_leg(a, torch, stream, nmol: int):
     import numpy as np
     from patmol_b200 import configs, gpu
     rng = np.random.default_rng(77)
-    sizes = rng.integers(3, 9, size=nmol)          # 3..8 atoms, uniform
+    sizes = rng.integers(3, a.batch_max_atoms + 1, size=nmol)   # uniform in 3..max atoms
     bases = [configs.organic_basis(int(k), 1000 + i, with_f=False) for i, k in enumerate(sizes)]
     gbs = [gpu.GpuBasis(bb, schwarz_tau=a.tau) for bb in bases]
     batch = gpu.GpuBatch(gbs)
@@ -185,7 +188,7 @@ def batched_leg(a, torch, stream, nmol: int):
     bufs = [batch.buffers(m) for m in range(nmol)]
 
     def timed(fn, reps):
-        for _ in range(max(a.warmup, 3)):
+        for _ in range(max(a.warmup, 1)):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -213,8 +216,8 @@ def batched_leg(a, torch, stream, nmol: int):
     for g in gbs:
         g.close()
     q = st["quartets"]
-    return {"workload": f"{nmol} seeded organic molecules (C/N/O/H walk), 3-8 atoms uniform, config-0 "
-                        "s/p/d basis, RHF Fock build of every molecule per step",
+    return {"workload": f"{nmol} seeded organic molecules (C/N/O/H walk), 3-{a.batch_max_atoms} atoms uniform, "
+                        "config-0 s/p/d basis, RHF Fock build of every molecule per step",
             "molecules": nmol, "basis_functions": int(sum(bb.norb for bb in bases)), "quartets": q,
             "graph_nodes": st["graph_nodes"],
             "ms_per_step_graph": t_graph, "ms_per_step_sequential": t_seq,
@@ -351,6 +354,13 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         stream = torch.cuda.Stream()
         torch.cuda.set_stream(stream)
+        if a.workload == "batch":
+            out = batched_leg(a, torch, stream, max(a.batch_molecules, 1))
+            out.update(metric="ERI quartets/s (batched Fock build)", value=out["quartets_per_s_graph"],
+                       unit="quartets/s", n_gpus=1, steps=max(1, min(a.steps, 5)), warmup=max(a.warmup, 1),
+                       higher_is_better=True, dtype="f64", data="synthetic")
+            print(json.dumps(out))
+            return
         leg = organic40_leg if a.workload == "organic40" else alkane_dpm_leg
         print(json.dumps(leg(a, torch, stream)))
         return

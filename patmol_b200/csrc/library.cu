@@ -451,7 +451,8 @@ __global__ void compact_kernel(const EriArgs a, unsigned long long *out, unsigne
 }
 
 // Compacted quartet lists (8 bytes per surviving quartet), when they fit in
-// half of the free device memory and PATGPU_LISTS is not 0: the class
+// half of the free device memory above a reserve of a tenth of the device
+// and PATGPU_LISTS is not 0: the class
 // kernels then visit only surviving quartets instead of stepping their
 // teams through screened-out items.  With mixed precision on, each class's
 // list is split into its FP64 and FP32 windows.
@@ -467,8 +468,15 @@ static int build_lists(patgpu_basis *h)
     }
     size_t fr = 0, tot = 0;
     PG_CUDA(cudaMemGetInfo(&fr, &tot));
+    // keep a tenth of the device (at least 4 GiB) out of reach of the lists,
+    // so that many handles (a batch) cannot starve each other's set-up
+    const size_t reserve = std::max<size_t>(tot / 10, (size_t)4 << 30);
+    const size_t room = fr > reserve ? (fr - reserve) / 2 : 0;
     const size_t bytes = sizeof(unsigned long long) * (size_t)std::max<long long>(total, 1);
-    if (bytes > h->d_list.bytes && bytes > fr / 2) return 0;
+    if (bytes > h->d_list.bytes && bytes > room) {
+        h->d_list.release();
+        return 0;
+    }
     PG_CUDA(h->d_list.ensure(bytes));
     const double lo = h->tau > 0.0 ? h->tau : -1.0;
     const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
