@@ -226,6 +226,30 @@ def batched_leg(a, torch, stream, nmol: int):
                       "speedup_vs_fp64_graph": t_graph / t_mixed, "max_abs_dG_vs_fp64": dG}}
 
 
+# ------------------------------------------------------------ SCF leg
+def scf_leg(torch):
+    """Water s/p/d (132 functions): full SCF to 1e-12 Eh through the GPU Fock
+    build, with full builds every iteration and with incremental
+    (density-difference, density-screened) builds; wall time per iteration
+    includes the host diagonalisation."""
+    from patmol_b200 import configs, gpu, scf
+    b = configs.water_spd()
+    out = {"workload": "water s/p/d (51 shells, 132 functions), RHF to 1e-12 Eh, DIIS"}
+    for name, inc in (("full", False), ("incremental", True)):
+        g = gpu.GpuBasis(b)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        r = scf.rhf(b, gpu=g, incremental=inc)
+        dt = time.time() - t0
+        out[name] = {"energy": r.energy, "iterations": r.iterations, "converged": r.converged,
+                     "seconds": dt, "s_per_iteration": dt / max(r.iterations, 1)}
+        if inc:
+            out[name]["quartets_per_iteration"] = r.quartets_computed
+        g.close()
+    out["dE_incremental_vs_full"] = out["incremental"]["energy"] - out["full"]["energy"]
+    return out
+
+
 # ------------------------------------------------------ other workloads
 def _timed_builds(torch, stream, G, P, Gd, reps):
     """Device-timed Fock builds (ms each) through patgpu_rhf_gmatrix_device."""
@@ -515,6 +539,8 @@ def main():
         }
         if world == 1 and a.batch_molecules > 0:
             line["batched"] = batched_leg(a, torch, stream, a.batch_molecules)
+        if world == 1:
+            line["scf"] = scf_leg(torch)
         if world == 1 and not a.no_cpu_baseline:
             res, err = reference_fock(2, 1)
             line["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -171,6 +171,18 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
 int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,
                         double *grad);
 
+/* Density-weighted screening (no counterpart in the reference, which
+ * screens nothing at run time): with tau_dens > 0 the host-buffer builds
+ * (patgpu_rhf_gmatrix, patgpu_uhf_gmatrix, patgpu_jk) skip every quartet
+ * whose bound Q_ab Q_cd max(4|D_ab|, 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|)
+ * (shell-block maxima of the build's density) is below tau_dens.  Meant for
+ * incremental builds G[P_n] = G[P_(n-1)] + G[P_n - P_(n-1)], whose density
+ * difference shrinks as the SCF converges.  Needs the compacted lists (a
+ * handle without them computes every quartet).  0 (the default) turns it
+ * off.  patgpu_last_computed: quartets computed by the last host-buffer build. */
+int patgpu_set_density_screening(patgpu_handle h, double tau_dens);
+int patgpu_last_computed(patgpu_handle h, long long *quartets);
+
 /* Batches (no counterpart in the reference, which runs one molecule per
  * process): many molecules advanced in lock step.  A batch holds the
  * molecules' handles (which must outlive it and must not be used
@@ -201,7 +213,9 @@ int patgpu_batch_last_timing(patgpu_batch b, double *kernel_ns);
  * product and sum stay FP64; their integrals are below tau_fp32 in size, so
  * the absolute error per integral is about 1e-7 tau_fp32.  0 turns it off
  * (the default).  patgpu_mixed_stats returns how many quartets of this
- * handle run in FP32. */
+ * handle run in FP32.  The FP32 window runs over the handle's compacted
+ * quartet lists; a handle without lists (not enough device memory, or
+ * PATGPU_LISTS=0) stays FP64 and reports 0. */
 int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32);
 int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32);
 

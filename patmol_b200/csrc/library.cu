@@ -114,6 +114,7 @@ struct ClassWork {
     int u0 = 0, nu = 0, v0 = 0, nv = 0, same = 0;   // bra and ket pair ranges
     long long total = 0;         // unscreened quartets of the class (all ranks)
     long long items = 0;         // work items of this rank: ceil((total - rank) / nranks)
+    int idx = 0;                 // position in the handle's work list
     // compacted lists: this class's survivors at [loff, loff + count) of the
     // handle's list, the FP64 window (bound >= tau_mix, or all without mixed
     // precision) first, nhi entries, then the FP32 window
@@ -151,6 +152,13 @@ struct patgpu_basis {
     long long nquart = 0, nquart_unscreened = 0;
     pg::DBuf d_list;                 // compacted class quartet indices (uint64), when lists are on
     bool lists = false;
+    // density-weighted screening of host-buffer builds (tau_dens > 0): the
+    // lists are filtered by Q_ab Q_cd max|D| against the build's density
+    double tau_dens = 0.0;
+    pg::DBuf d_soff, d_snst, d_dsh, d_flist, d_fcnt;
+    std::vector<unsigned long long> fcnt;   // per class: filtered FP64-window, FP32-window counts
+    bool filtered = false;                  // the current build runs over d_flist
+    long long last_computed = 0;            // quartets computed by the last host-buffer build
     // work buffers
     pg::DBuf d_D0, d_D1, d_A0, d_A1, d_Pk0, d_Pk1, d_Gk0, d_Gk1, d_err;
     std::vector<double> h_stage;
@@ -377,6 +385,12 @@ static EriArgs class_args(const patgpu_basis *h, const ClassWork &w, int mode, d
 static EriArgs list_args(const patgpu_basis *h, const ClassWork &w, int mode, int window)
 {
     EriArgs a = class_args(h, w, mode, -1.0, INFINITY);
+    if (h->filtered && window != 2) {   // density-screened sublists of this build
+        const unsigned long long *l = h->d_flist.as<unsigned long long>() + w.loff;
+        a.klist = window == 1 ? l + w.nhi : l;
+        a.nquart = (long long)h->fcnt[2 * w.idx + window];
+        return a;
+    }
     const unsigned long long *l = h->d_list.as<unsigned long long>() + w.loff;
     a.klist = window == 1 ? l + w.nhi : l;
     a.nquart = window == 0 ? w.nhi : (window == 1 ? w.count - w.nhi : w.count);
@@ -406,16 +420,15 @@ static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const 
         return a.nquart > 0 ? launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant32)
                             : cudaSuccess;
     }
-    EriArgs a = class_args(h, w, proto.mode, mixed ? h->tau_mix : lo, INFINITY);
+    // without lists every class runs FP64 over its whole window: a second
+    // (FP32) pass over the implicit space would step every team through
+    // all of the class's items again and cost more than it saves
+    EriArgs a = class_args(h, w, proto.mode, lo, INFINITY);
     a.D0 = proto.D0;
     a.D1 = proto.D1;
     a.A0 = proto.A0;
     a.A1 = proto.A1;
-    cudaError_t e = launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant);
-    if (e != cudaSuccess || !mixed) return e;
-    a.tau_lo = lo;
-    a.tau_hi = h->tau_mix;
-    return launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant32);
+    return launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant);
 }
 
 __global__ void count_kernel(const EriArgs a, unsigned long long *cnt)
@@ -565,6 +578,7 @@ static int build_quartets(patgpu_basis *h)
         owned += all[k].count;
         if (all[k].count) h->work.push_back(all[k]);
     }
+    for (size_t k = 0; k < h->work.size(); ++k) h->work[k].idx = (int)k;
     h->nquart = owned;
     h->nquart_unscreened = unscreened;
     return build_lists(h);
@@ -774,6 +788,99 @@ static int record_timing(patgpu_basis *h)
     return 0;
 }
 
+// Largest |D_ij| over the component block of every shell pair (both
+// densities when D1 is set); shells without components give 0.
+__global__ void shell_dmax_kernel(const double *__restrict__ D0, const double *__restrict__ D1, int n,
+                                  const int *__restrict__ soff, const int *__restrict__ snst, int nsh,
+                                  double *__restrict__ dsh)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nsh * nsh; idx += gridDim.x * blockDim.x) {
+        const int s1 = idx / nsh, s2 = idx - (idx / nsh) * nsh;
+        double m = 0.0;
+        for (int i = 0; i < snst[s1]; ++i)
+            for (int j = 0; j < snst[s2]; ++j) {
+                const size_t o = (size_t)(soff[s1] + i) * n + soff[s2] + j;
+                m = fmax(m, fabs(D0[o]));
+                if (D1) m = fmax(m, fabs(D1[o]));
+            }
+        dsh[idx] = m;
+    }
+}
+
+// Keep the list entries whose contribution bound Q_ab Q_cd max(4|D_ab|,
+// 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|) reaches tau (shell-block maxima;
+// the factor 4 covers the Coulomb weight), appended with warp-aggregated
+// atomics.
+__global__ void density_filter_kernel(const EriArgs a, const double *__restrict__ dsh, int nsh, double tau,
+                                      unsigned long long *out, unsigned long long *cnt)
+{
+    for (long long qi0 = (long long)blockIdx.x * blockDim.x; qi0 < a.nquart;
+         qi0 += (long long)gridDim.x * blockDim.x) {
+        const long long qi = qi0 + threadIdx.x;
+        int u = 0, v = 0;
+        bool keep = qi < a.nquart && eri_quartet_at(a, qi, u, v);
+        if (keep) {
+            const int sa = a.pr.sa[u], sb = a.pr.sb[u], sc = a.pr.sa[v], sd = a.pr.sb[v];
+            const double dj = 4.0 * fmax(dsh[sa * nsh + sb], dsh[sc * nsh + sd]);
+            const double dk = fmax(fmax(dsh[sa * nsh + sc], dsh[sa * nsh + sd]), fmax(dsh[sb * nsh + sc], dsh[sb * nsh + sd]));
+            keep = a.Q[u] * a.Q[v] * fmax(dj, dk) >= tau;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (!m) continue;
+        const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+        unsigned long long base = 0;
+        if (lane == lead) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (keep) out[base + __popc(m & ((1u << lane) - 1u))] = a.klist[qi];
+    }
+}
+
+// Filter every class's list(s) against the density of this build (d_D0, and
+// d_D1 for UHF) into d_flist; host_fock then launches over the sublists.
+static int density_filter(patgpu_basis *h, bool two)
+{
+    cudaStream_t s = h->stream;
+    if (!h->d_soff.p) {
+        std::vector<int> soff(h->nsh), snst(h->nsh);
+        for (int i = 0; i < h->nsh; ++i) {
+            soff[i] = h->off[i];
+            snst[i] = h->nst[i];
+        }
+        PG_CUDA(upload(h->d_soff, soff, s));
+        PG_CUDA(upload(h->d_snst, snst, s));
+    }
+    const int nsh = h->nsh;
+    PG_CUDA(h->d_dsh.ensure(sizeof(double) * (size_t)nsh * nsh));
+    shell_dmax_kernel<<<grid_for((long long)nsh * nsh, h->num_sms), 256, 0, s>>>(
+        h->d_D0.as<double>(), two ? h->d_D1.as<double>() : nullptr, h->n, h->d_soff.as<int>(), h->d_snst.as<int>(),
+        nsh, h->d_dsh.as<double>());
+    PG_CUDA(h->d_flist.ensure(std::max<size_t>(h->d_list.bytes, 16)));
+    const size_t nc = 2 * std::max<size_t>(h->work.size(), 1);
+    PG_CUDA(h->d_fcnt.ensure(sizeof(unsigned long long) * nc));
+    PG_CUDA(cudaMemsetAsync(h->d_fcnt.p, 0, sizeof(unsigned long long) * nc, s));
+    const double lo = h->tau > 0.0 ? h->tau : -1.0;
+    const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
+    unsigned long long *out = h->d_flist.as<unsigned long long>();
+    for (const auto &w : h->work)
+        for (int win = 0; win < (mixed ? 2 : 1); ++win) {
+            EriArgs a = list_args(h, w, MODE_RHF, win);
+            if (a.nquart <= 0) continue;
+            const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
+            density_filter_kernel<<<std::max(g, 1), 256, 0, s>>>(a, h->d_dsh.as<double>(), nsh, h->tau_dens,
+                                                                  out + w.loff + (win ? w.nhi : 0),
+                                                                  h->d_fcnt.as<unsigned long long>() + 2 * w.idx + win);
+        }
+    PG_CUDA(cudaGetLastError());
+    h->fcnt.assign(nc, 0);
+    PG_CUDA(cudaMemcpyAsync(h->fcnt.data(), h->d_fcnt.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    h->filtered = true;
+    long long tot = 0;
+    for (auto c : h->fcnt) tot += (long long)c;
+    h->last_computed = tot;
+    return 0;
+}
+
 // Host-buffer Fock build shared by the RHF / UHF / JK entry points.
 static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *P1, double *G0, double *G1)
 {
@@ -792,7 +899,16 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
     }
     PG_CUDA(cudaMemsetAsync(h->d_A0.p, 0, sizeof(double) * nn, s));
     if (two) PG_CUDA(cudaMemsetAsync(h->d_A1.p, 0, sizeof(double) * nn, s));
+    h->last_computed = h->nquart;
+    if (h->tau_dens > 0.0 && h->lists) {
+        rc = density_filter(h, mode == MODE_UHF);
+        if (rc) {
+            h->filtered = false;
+            return rc;
+        }
+    }
     rc = launch_fock(h, mode, s);
+    h->filtered = false;
     if (rc) return rc;
     finish_kernel<<<grid_for((long long)no2, h->num_sms), 256, 0, s>>>(h->d_A0.as<double>(), h->d_Gk0.as<double>(),
                                                                       h->n);
@@ -1212,7 +1328,12 @@ int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
     PG_CUDA(cudaStreamSynchronize(h->stream));
     h->nquart_fp32 = (long long)c;
     int rc = h->lists ? build_lists(h) : 0;
-    return rc ? rc : tune_fp32(h);
+    if (rc) return rc;
+    if (!h->lists) {   // mixed precision runs over the compacted lists only
+        h->nquart_fp32 = 0;
+        return 0;
+    }
+    return tune_fp32(h);
 }
 
 int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32)
@@ -1287,6 +1408,20 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
     if (rc) return rc;
     return run_oneints(nshell, l, cen, off, nst, prim_off, alpha, coef, ncen, charge, xyz, skipcen, n, S, T, H, Hdpm,
                        nullptr);
+}
+
+int patgpu_set_density_screening(patgpu_handle h, double tau_dens)
+{
+    if (!h || !(tau_dens >= 0.0)) return fail(PATGPU_EINVAL, "bad density-screening threshold");
+    h->tau_dens = tau_dens;
+    return 0;
+}
+
+int patgpu_last_computed(patgpu_handle h, long long *quartets)
+{
+    if (!h || !quartets) return fail(PATGPU_EINVAL, "null argument");
+    *quartets = h->last_computed;
+    return 0;
 }
 
 int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,

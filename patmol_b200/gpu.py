@@ -70,6 +70,8 @@ def lib():
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_mixed_stats.argtypes = [H, lp]
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.patgpu_set_density_screening.argtypes = [H, ctypes.c_double]
+        L.patgpu_last_computed.argtypes = [H, lp]
         L.patgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(H), ctypes.POINTER(H)]
         L.patgpu_batch_destroy.argtypes = [H]
         L.patgpu_batch_buffers.argtypes = [H, ctypes.c_int, ctypes.POINTER(dp), ctypes.POINTER(dp)]
@@ -214,6 +216,16 @@ class GpuBasis:
         _check(lib().patgpu_rhf_gradient(self.h, _p(P), Wp, int(parts), int(bool(with_dpm)), _p(g)),
                "patgpu_rhf_gradient")
         return g.reshape(-1, 3)
+
+    def set_density_screening(self, tau_dens: float):
+        """Skip quartets with Q_ab Q_cd max|D| < tau_dens in host-buffer builds
+        (for incremental builds over density differences); 0 turns it off."""
+        _check(lib().patgpu_set_density_screening(self.h, float(tau_dens)), "set_density_screening")
+
+    def last_computed(self) -> int:
+        n = ctypes.c_longlong()
+        _check(lib().patgpu_last_computed(self.h, ctypes.byref(n)), "patgpu_last_computed")
+        return n.value
 
     def set_mixed_precision(self, tau_fp32: float) -> int:
         """FP32 arithmetic for quartets with Schwarz bound below tau_fp32

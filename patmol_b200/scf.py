@@ -46,6 +46,7 @@ class RHFResult:
     iterations: int
     converged: bool
     enuc: float
+    quartets_computed: list | None = None   # per iteration, incremental builds
 
 
 def orthogonalizer(S: np.ndarray, smin: float = 1e-10) -> np.ndarray:
@@ -135,14 +136,49 @@ def _setup(gb: GpuBasis, dpm: bool):
     return Sp, Hp
 
 
+class IncrementalFock:
+    """G[P_n] = G[P_(n-1)] + G[P_n - P_(n-1)] with the density-screened
+    difference build (patgpu_set_density_screening at tau_inc; the default
+    1e-14 drops contributions at the level below which the reference stores
+    no integral, twoints.c:375), and a full unscreened build every
+    `full_every` iterations.  Records the quartets each build computed."""
+
+    def __init__(self, gb: GpuBasis, tau_inc: float = 1e-14, full_every: int = 8):
+        self.gb, self.tau_inc, self.full_every = gb, tau_inc, full_every
+        self.P = self.G = None
+        self.n = 0
+        self.computed = []
+
+    def __call__(self, Pp, full: bool = False):
+        gb = self.gb
+        if full or self.G is None or self.n % self.full_every == 0:
+            gb.set_density_screening(0.0)
+            G = gb.rhf_form_gmatrix(Pp)
+        else:
+            gb.set_density_screening(self.tau_inc)
+            G = self.G + gb.rhf_form_gmatrix(Pp - self.P)
+            gb.set_density_screening(0.0)
+        self.computed.append(gb.last_computed())
+        self.n += 1
+        self.P, self.G = Pp.copy(), G
+        return G
+
+
 def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
-        maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8) -> RHFResult:
+        maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
+        tau_inc: float = 1e-14) -> RHFResult:
+    """Closed-shell SCF.  incremental=True builds G from density differences
+    (IncrementalFock) during the iterations; the final energy always comes
+    from a full build."""
     gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
     Sp, Hp = _setup(gb, dpm)
     st = _RHFState(basis, Sp, Hp, ndiis, conv)
+    fock = IncrementalFock(gb, tau_inc) if incremental else None
     while st.it < maxit and not st.converged:
-        st.step(gb.rhf_form_gmatrix(st.packed_density()))
+        Pp = st.packed_density()
+        st.step(fock(Pp) if fock else gb.rhf_form_gmatrix(Pp))
     res = st.finish(gb.rhf_form_gmatrix(st.packed_density()))
+    res.quartets_computed = fock.computed if fock else None
     if gpu is None:
         gb.close()
     return res

@@ -35,3 +35,15 @@ def test_variant_matches_oracle(water_ref, variant, monkeypatch):
     G = g.rhf_form_gmatrix(P)
     assert np.abs(G - ref).max() < 1e-11
     g.close()
+
+
+def test_implicit_enumeration_without_lists(water_ref, monkeypatch):
+    """PATGPU_LISTS=0: the kernels screen the implicit quartet space on the
+    fly; same G, and mixed precision stays off (FP32 runs over lists only)."""
+    b, P, ref = water_ref
+    monkeypatch.setenv("PATGPU_LISTS", "0")
+    g = gpu.GpuBasis(b)
+    assert np.abs(g.rhf_form_gmatrix(P) - ref).max() < 1e-11
+    assert g.set_mixed_precision(1e-8) == 0
+    assert np.abs(g.rhf_form_gmatrix(P) - ref).max() < 1e-11
+    g.close()
