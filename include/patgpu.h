@@ -26,6 +26,7 @@
 #define PATGPU_H
 #include <stddef.h>
 #include <stdint.h>
+#include <stdio.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -170,6 +171,28 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
 #define PATGPU_GRAD_ALL 7
 int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,
                         double *grad);
+
+/* The reference's ERI files from the GPU integrals: the record stream of
+ * two_electron_ints (twoints.c:188-418) -- 16-byte ERINT records
+ * (erifs.h:19-22) of every canonical function quartet with |v| > 1e-14, in
+ * the reference's shell-quartet and component order, MPI rank `rank` of
+ * `nproc` taking the reference's card-dealt share (twoints.c:280-288), a
+ * new file after max_records records (the reference uses
+ * MAXFILESIZE / 16, pconfig.h:7).  For callers that keep the reference's
+ * file-reading G build (rhf_form_gmatrix in scfaux.c, e.g. in patmpi) and
+ * only take the integrals from the GPU.  patgpu_write_eri_files names the
+ * files prefix + rank + file number + basename, as create_filename does
+ * (erifs.c:54-73); patgpu_write_eri_files_with opens them through the
+ * caller's function (the reference's createERIFile, erifs.c:84-90).
+ * numints[f] receives file f's record count (capacity max_files), *nfiles
+ * the file count.  The drop-in two_electron_ints writes them too when
+ * PATGPU_ERI_FILES=1. */
+int patgpu_write_eri_files(patgpu_handle h, int start, int rank, int nproc, const char *prefix,
+                           const char *basename, long long max_records, int max_files, int *numints, int *nfiles);
+int patgpu_write_eri_files_with(patgpu_handle h, int start, int rank, int nproc,
+                                FILE *(*open_file)(int rank, int file_no, const char *basename),
+                                const char *basename, long long max_records, int max_files, int *numints,
+                                int *nfiles);
 
 /* Density-weighted screening (no counterpart in the reference, which
  * screens nothing at run time): with tau_dens > 0 the host-buffer builds

@@ -8,6 +8,7 @@
 // points report the missing accessors through fatalError.
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -31,6 +32,7 @@ int number_of_shells() __attribute__((weak));
 int number_of_centers() __attribute__((weak));
 int skip_center() __attribute__((weak));
 void fatalError(const char *message) __attribute__((weak));
+FILE *createERIFile(int rank, int file_no, const char *bname) __attribute__((weak));   // erifs.c:84-90
 }
 
 namespace {
@@ -143,6 +145,20 @@ void two_electron_ints(ERIFS *tfiles, int start)
     if (patgpu_set_quartets(h, start, rank % nproc, nproc)) die("two_electron_ints");
     g_handles[tfiles] = h;
     tfiles->nfiles = 0;   // integral-direct: no ERI files
+    // PATGPU_ERI_FILES=1: also write the reference's ERI files, for a host
+    // program whose own file-reading G build stays linked
+    const char *ef = getenv("PATGPU_ERI_FILES");
+    if (ef && !strcmp(ef, "1")) {
+        if (!createERIFile) die("PATGPU_ERI_FILES=1 needs the host program's createERIFile");
+        int nf = 0;
+        if (patgpu_write_eri_files_with(h, start, rank % nproc, nproc, createERIFile, tfiles->basename,
+                                        (1LL << 30) / 16, 1 << 20, tfiles->numints, &nf))
+            die("two_electron_ints: writing the ERI files");
+        tfiles->nfiles = nf;
+        long long nrec = 0;
+        for (int f = 0; f < nf; ++f) nrec += tfiles->numints[f];
+        fprintf(stderr, "patgpu: wrote %d ERI file(s), %lld records\n", nf, nrec);
+    }
 }
 
 void rhf_form_gmatrix(const ERIFS *tfiles, const double *Pmat, double *Gmat)

@@ -1272,6 +1272,164 @@ int patgpu_eri_quartets(patgpu_handle h, int nq, const int *sh4, double *out)
     return 0;
 }
 
+// ------------------------------------------------------------ ERI files
+}  // extern "C"
+namespace pg {
+
+// One record of the reference's ERI files: the layout of ERINT
+// (erifs.h:19-22), a double and four unsigned short function indices,
+// 16-byte aligned.
+struct ErintRecord {
+    double val;
+    unsigned short i, j, k, l;
+};
+static_assert(sizeof(ErintRecord) == 16, "ERINT record layout");
+
+// The reference's file stream of two_electron_ints (twoints.c:188-418),
+// with the integrals from the GPU: shell quartets in its loop order
+// (ish >= start, jsh <= ish, ksh <= ish, lsh <= ksh), on MPI rank r of nproc
+// the quartets q with (q + 1) % nproc == r (the card dealing of
+// twoints.c:280-288), inside each quartet the component order and the
+// canonical restriction of twoints.c:316-337 (j <= i, k <= i, l <= k, and
+// l <= j when i = k), records with |v| > 1e-14 (twoints.c:374-379), and a
+// new file once a file holds more than max_records (twoints.c:380-386).
+// Quartets whose Schwarz bound is below the handle's threshold are skipped
+// only when that threshold is at most 1e-14 (then none of their integrals
+// reaches the record threshold).  open_file(f) returns file f for writing.
+template <class OpenFile>
+static int write_eri_stream(patgpu_basis *h, int start, int rank, int nproc, long long max_records,
+                            OpenFile open_file, int max_files, int *numints, int *nfiles)
+{
+    if (h->n > 65536) return fail(PATGPU_EINVAL, "ERI records hold 16-bit function indices; n = %d", h->n);
+    const int nsh = h->nsh;
+    std::vector<int> pidx((size_t)nsh * nsh, -1);
+    for (int u = 0; u < h->npair; ++u) {
+        pidx[(size_t)h->psa[u] * nsh + h->psb[u]] = u;
+        pidx[(size_t)h->psb[u] * nsh + h->psa[u]] = u;
+    }
+    const bool screen = h->tau > 0.0 && h->tau <= 1e-14;
+    const double threshold = 1e-14;
+    int nf = 0;
+    long long fsize = 0;
+    FILE *out = open_file(0);
+    if (!out) return fail(PATGPU_EINVAL, "cannot create ERI file 0");
+    std::vector<int> batch;           // 4 shells per quartet
+    std::vector<double> vals;
+    long long batch_vals = 0;
+    const long long kBatchVals = 1LL << 24;   // 128 MiB of integrals per GPU round trip
+    std::vector<ErintRecord> recs;
+    int rc = 0;
+    auto flush = [&]() -> int {
+        const int nq = (int)(batch.size() / 4);
+        if (!nq) return 0;
+        vals.resize((size_t)batch_vals);
+        int r = patgpu_eri_quartets(h, nq, batch.data(), vals.data());
+        if (r) return r;
+        size_t o = 0;
+        for (int q = 0; q < nq; ++q) {
+            const int *sq = batch.data() + 4 * q;
+            const int n0 = h->nst[sq[0]], n1 = h->nst[sq[1]], n2 = h->nst[sq[2]], n3 = h->nst[sq[3]];
+            const int o0 = h->off[sq[0]], o1 = h->off[sq[1]], o2 = h->off[sq[2]], o3 = h->off[sq[3]];
+            recs.clear();
+            for (int a = 0; a < n0; ++a) {
+                const int ir = o0 + a;
+                for (int b = 0; b < n1; ++b) {
+                    const int jr = o1 + b;
+                    if (jr > ir) break;
+                    for (int c = 0; c < n2; ++c) {
+                        const int kr = o2 + c;
+                        if (kr > ir) break;
+                        for (int d = 0; d < n3; ++d) {
+                            const int lr = o3 + d;
+                            if (lr > kr) break;
+                            if (ir == kr && lr > jr) break;
+                            const double v = vals[o + (((size_t)a * n1 + b) * n2 + c) * n3 + d];
+                            if (std::fabs(v) > threshold)
+                                recs.push_back({v, (unsigned short)ir, (unsigned short)jr, (unsigned short)kr,
+                                                (unsigned short)lr});
+                        }
+                    }
+                }
+            }
+            o += (size_t)n0 * n1 * n2 * n3;
+            if (!recs.empty() && std::fwrite(recs.data(), sizeof(ErintRecord), recs.size(), out) != recs.size())
+                return fail(PATGPU_EINVAL, "writing ERI file %d failed", nf);
+            fsize += (long long)recs.size();
+            if (fsize > max_records) {
+                std::fclose(out);
+                if (nf >= max_files) return fail(PATGPU_EINVAL, "more than %d ERI files", max_files);
+                numints[nf++] = (int)fsize;
+                out = open_file(nf);
+                if (!out) return fail(PATGPU_EINVAL, "cannot create ERI file %d", nf);
+                fsize = 0;
+            }
+        }
+        batch.clear();
+        batch_vals = 0;
+        return 0;
+    };
+    long long pknt = 0;
+    for (int ish = start; ish < nsh && !rc; ++ish)
+        for (int jsh = 0; jsh <= ish && !rc; ++jsh)
+            for (int ksh = 0; ksh <= ish && !rc; ++ksh)
+                for (int lsh = 0; lsh <= ksh && !rc; ++lsh) {
+                    ++pknt;
+                    if (nproc > 1 && pknt % nproc != rank) continue;
+                    if (nproc > 1) pknt = rank;
+                    if (!h->nst[ish] || !h->nst[jsh] || !h->nst[ksh] || !h->nst[lsh]) continue;
+                    if (screen) {
+                        const int u = pidx[(size_t)ish * nsh + jsh], v = pidx[(size_t)ksh * nsh + lsh];
+                        if (h->Q[u] * h->Q[v] < h->tau) continue;
+                    }
+                    batch.insert(batch.end(), {ish, jsh, ksh, lsh});
+                    batch_vals += (long long)h->nst[ish] * h->nst[jsh] * h->nst[ksh] * h->nst[lsh];
+                    if (batch_vals >= kBatchVals) rc = flush();
+                }
+    if (!rc) rc = flush();
+    if (rc) {
+        std::fclose(out);
+        return rc;
+    }
+    std::fclose(out);
+    if (fsize) {
+        if (nf >= max_files) return fail(PATGPU_EINVAL, "more than %d ERI files", max_files);
+        numints[nf++] = (int)fsize;
+    }
+    *nfiles = nf;
+    return 0;
+}
+
+}  // namespace pg
+extern "C" {
+
+int patgpu_write_eri_files(patgpu_handle h, int start, int rank, int nproc, const char *prefix,
+                           const char *basename, long long max_records, int max_files, int *numints, int *nfiles)
+{
+    if (!h || start < 0 || nproc < 1 || rank < 0 || rank >= nproc || !prefix || !basename || max_records < 1 ||
+        max_files < 1 || !numints || !nfiles)
+        return fail(PATGPU_EINVAL, "patgpu_write_eri_files: bad argument");
+    if (rank > 99999) return fail(PATGPU_EINVAL, "rank too large for the ERI file names");
+    const std::string pre(prefix), base(basename);
+    auto open_file = [&](int f) -> FILE * {
+        if (f > 99999) return nullptr;
+        const std::string name = pre + std::to_string(rank) + std::to_string(f) + base;   // erifs.c:54-73
+        return std::fopen(name.c_str(), "wb");
+    };
+    return write_eri_stream(h, start, rank, nproc, max_records, open_file, max_files, numints, nfiles);
+}
+
+int patgpu_write_eri_files_with(patgpu_handle h, int start, int rank, int nproc,
+                                FILE *(*open_file)(int rank, int file_no, const char *basename),
+                                const char *basename, long long max_records, int max_files, int *numints,
+                                int *nfiles)
+{
+    if (!h || start < 0 || nproc < 1 || rank < 0 || rank >= nproc || !open_file || !basename || max_records < 1 ||
+        max_files < 1 || !numints || !nfiles)
+        return fail(PATGPU_EINVAL, "patgpu_write_eri_files_with: bad argument");
+    auto of = [&](int f) -> FILE * { return open_file(rank, f, basename); };
+    return write_eri_stream(h, start, rank, nproc, max_records, of, max_files, numints, nfiles);
+}
+
 int patgpu_select_device(int index)
 {
     int ndev = 0;

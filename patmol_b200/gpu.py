@@ -70,6 +70,8 @@ def lib():
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_mixed_stats.argtypes = [H, lp]
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.patgpu_write_eri_files.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                             ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ip, ip]
         L.patgpu_set_density_screening.argtypes = [H, ctypes.c_double]
         L.patgpu_last_computed.argtypes = [H, lp]
         L.patgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(H), ctypes.POINTER(H)]
@@ -217,6 +219,17 @@ class GpuBasis:
                "patgpu_rhf_gradient")
         return g.reshape(-1, 3)
 
+    def write_eri_files(self, prefix: str, basename: str, start: int = 0, rank: int = 0, nproc: int = 1,
+                        max_records: int = (1 << 30) // 16, max_files: int = 4096):
+        """Write the reference's ERI files (patgpu_write_eri_files); returns the
+        record count of each file, named prefix + rank + file number + basename."""
+        numints = np.zeros(max_files, dtype=np.int32)
+        nf = ctypes.c_int()
+        _check(lib().patgpu_write_eri_files(self.h, start, rank, nproc, prefix.encode(), basename.encode(),
+                                            int(max_records), max_files, _p(numints, ctypes.c_int),
+                                            ctypes.byref(nf)), "patgpu_write_eri_files")
+        return [int(x) for x in numints[:nf.value]]
+
     def set_density_screening(self, tau_dens: float):
         """Skip quartets with Q_ab Q_cd max|D| < tau_dens in host-buffer builds
         (for incremental builds over density differences); 0 turns it off."""
@@ -307,6 +320,15 @@ class GpuBatch:
         v = ctypes.c_double()
         _check(lib().patgpu_batch_last_timing(self.b, ctypes.byref(v)), "patgpu_batch_last_timing")
         return v.value
+
+
+ERINT_DTYPE = np.dtype([("val", "<f8"), ("i", "<u2"), ("j", "<u2"), ("k", "<u2"), ("l", "<u2")])
+
+
+def read_eri_files(prefix: str, basename: str, rank: int, nfiles: int):
+    """Concatenated records of ERI files f = 0 .. nfiles-1 (ERINT layout, erifs.h:19-22)."""
+    parts = [np.fromfile(f"{prefix}{rank}{f}{basename}", dtype=ERINT_DTYPE) for f in range(nfiles)]
+    return np.concatenate(parts) if parts else np.zeros(0, dtype=ERINT_DTYPE)
 
 
 def onebody(basis, want_sth=True, Hdpm=None):

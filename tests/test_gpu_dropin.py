@@ -3,6 +3,7 @@ module, linear algebra) linked against libpatgpu.so in place of twoints.c,
 dpmints.c, oneints.c, rys.c and scfaux.c's two G builds (oracle/Makefile,
 target `dropin`).  Converged energies against the reference's."""
 import os
+import re
 import shutil
 import subprocess
 
@@ -45,3 +46,19 @@ def test_dropin_sf6_fixture(tmp_path, golden_meta):
     vals, _ = run_dropin(tmp_path, patin=os.path.join(GOLDEN, "sf6_patin.dat"))
     g = golden_meta["sf6"]
     assert abs(vals[1] - g["e_total"]) < 1e-5, (vals[1], g["e_total"])
+
+
+def test_dropin_writes_reference_eri_files(tmp_path, golden_meta):
+    """PATGPU_ERI_FILES=1: two_electron_ints also writes the reference's ERI
+    files through the host program's createERIFile and reports them in the
+    ERIFS handle; the reference's own clean-up (clean_ERIFS, erifs.c:68-81)
+    then finds and removes every one of them, and the SCF is unchanged.  The
+    files' contents are checked in test_gpu_erifiles.py."""
+    vals, err = run_dropin(tmp_path, configs.water_spd(), env={"PATGPU_ERI_FILES": "1"})
+    assert abs(vals[1] - golden_meta["water_spd"]["e_total_exact_integrals"]) < 5e-9
+    m = re.search(r"patgpu: wrote (\d+) ERI file\(s\), (\d+) records", err)
+    assert m and int(m.group(1)) >= 1 and int(m.group(2)) > 1.7e7, err[-500:]
+    # <rank><file number>MINTS.DAT (erifs.c:54-73); MOMINTS.DAT is the
+    # reference's moment-integral file, not an ERI file
+    left = [p for p in os.listdir(tmp_path) if re.fullmatch(r"\d+MINTS\.DAT", p)]
+    assert not left, left
