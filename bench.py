@@ -250,6 +250,40 @@ def scf_leg(torch):
     return out
 
 
+def linalg_leg():
+    """The SCF step after the Fock build (X^T F X, eigenpairs, C = X V,
+    P = C_occ C_occ^T, W) at the largest config-3 molecule's size (1056
+    functions) and at config 2's (2560): the GPU (patgpu_scf_density_host,
+    host buffers in and out) against numpy on the host (threads as numpy
+    uses them).  Seeded symmetric F, X = 1."""
+    import numpy as np
+    from patmol_b200 import gpu
+    out = {"workload": "SCF density step, seeded symmetric F, X = identity, nocc = n/8"}
+    for n in (1056, 2560):
+        rng = np.random.default_rng(n)
+        A = rng.normal(size=(n, n))
+        F = (A + A.T) / 2
+        il = np.tril_indices(n)
+        Fp = F[il].copy()
+        X = np.eye(n)
+        nocc = n // 8
+        t0 = time.time()
+        e, V = np.linalg.eigh(X.T @ F @ X)
+        C = X @ V
+        P = C[:, :nocc] @ C[:, :nocc].T
+        W = (C[:, :nocc] * e[:nocc]) @ C[:, :nocc].T
+        t_host = time.time() - t0
+        la = gpu.GpuScfLinalg(X, nocc)
+        la.density(Fp)                       # warm-up
+        t0 = time.time()
+        eg, _, Pg, Wg = la.density(Fp)
+        t_dev = time.time() - t0
+        la.close()
+        out[str(n)] = {"host_s": t_host, "gpu_s": t_dev, "speedup": t_host / t_dev,
+                       "max_abs_dP": float(np.abs(Pg - P[il]).max()), "max_abs_deps": float(np.abs(eg - e).max())}
+    return out
+
+
 # ------------------------------------------------------ other workloads
 def _timed_builds(torch, stream, G, P, Gd, reps):
     """Device-timed Fock builds (ms each) through patgpu_rhf_gmatrix_device."""
@@ -541,6 +575,7 @@ def main():
             line["batched"] = batched_leg(a, torch, stream, a.batch_molecules)
         if world == 1:
             line["scf"] = scf_leg(torch)
+            line["linalg"] = linalg_leg()
         if world == 1 and not a.no_cpu_baseline:
             res, err = reference_fock(2, 1)
             line["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -194,6 +194,25 @@ int patgpu_write_eri_files_with(patgpu_handle h, int start, int rank, int nproc,
                                 const char *basename, long long max_records, int max_files, int *numints,
                                 int *nfiles);
 
+/* SCF linear algebra on the GPU (the reference does it on the host:
+ * spack_trans, spack_diag, form_cmatrix, form_pmatrix; rhfscf.c:36-47).
+ * patgpu_scf_create takes the orthogonaliser X (host, n x nx, row-major --
+ * the reference's xmat, or any X with X^T S X = 1) and the occupied-orbital
+ * count, and allocates every work array once.  patgpu_scf_density takes a
+ * packed Fock matrix on the device and forms F' = X^T F X, its eigenpairs
+ * (cuSOLVER syevd, ascending), C = X V and the packed half density
+ * P = C_occ C_occ^T on the device; optionally W = C_occ e_occ C_occ^T
+ * (device, packed), the eigenvalues (host, nx) and C (host, n x nx
+ * column-major, i.e. C[i + n a] is orbital a on function i).  It
+ * synchronises `stream` before returning. */
+typedef struct patgpu_scf_s *patgpu_scf;
+int patgpu_scf_create(int n, int nx, int nocc, const double *X, patgpu_scf *out);
+int patgpu_scf_destroy(patgpu_scf s);
+int patgpu_scf_density(patgpu_scf s, const double *dF, double *dP, double *dW, double *eps, double *C,
+                       void *stream);
+/* The same with packed host buffers (F in; P and, if not NULL, W out). */
+int patgpu_scf_density_host(patgpu_scf s, const double *F, double *P, double *W, double *eps, double *C);
+
 /* Density-weighted screening (no counterpart in the reference, which
  * screens nothing at run time): with tau_dens > 0 the host-buffer builds
  * (patgpu_rhf_gmatrix, patgpu_uhf_gmatrix, patgpu_jk) skip every quartet

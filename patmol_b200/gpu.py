@@ -72,6 +72,9 @@ def lib():
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
         L.patgpu_write_eri_files.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                              ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ip, ip]
+        L.patgpu_scf_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ctypes.POINTER(H)]
+        L.patgpu_scf_destroy.argtypes = [H]
+        L.patgpu_scf_density_host.argtypes = [H, dp, dp, dp, dp, dp]
         L.patgpu_set_density_screening.argtypes = [H, ctypes.c_double]
         L.patgpu_last_computed.argtypes = [H, lp]
         L.patgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(H), ctypes.POINTER(H)]
@@ -320,6 +323,41 @@ class GpuBatch:
         v = ctypes.c_double()
         _check(lib().patgpu_batch_last_timing(self.b, ctypes.byref(v)), "patgpu_batch_last_timing")
         return v.value
+
+
+class GpuScfLinalg:
+    """SCF linear algebra on the GPU (patgpu_scf_*): from a Fock matrix, the
+    orbitals, the half density P and the energy-weighted density W."""
+
+    def __init__(self, X, nocc: int):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        self.n, self.nx = X.shape
+        self.nocc = nocc
+        s = ctypes.c_void_p()
+        _check(lib().patgpu_scf_create(self.n, self.nx, nocc, _p(X), ctypes.byref(s)), "patgpu_scf_create")
+        self.s = s
+
+    def close(self):
+        if self.s:
+            lib().patgpu_scf_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def density(self, F_packed):
+        """Returns (eps, C (n x nx), P packed, W packed)."""
+        F = np.ascontiguousarray(F_packed, dtype=np.float64)
+        no2 = self.n * (self.n + 1) // 2
+        P, W = np.empty(no2), np.empty(no2)
+        eps = np.empty(self.nx)
+        Ccm = np.empty((self.nx, self.n))
+        _check(lib().patgpu_scf_density_host(self.s, _p(F), _p(P), _p(W), _p(eps), _p(Ccm)),
+               "patgpu_scf_density_host")
+        return eps, Ccm.T.copy(), P, W
 
 
 ERINT_DTYPE = np.dtype([("val", "<f8"), ("i", "<u2"), ("j", "<u2"), ("k", "<u2"), ("l", "<u2")])

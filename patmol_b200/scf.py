@@ -20,7 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from .basis import Basis, pack, unpack
-from .gpu import GpuBasis, GpuBatch
+from .gpu import GpuBasis, GpuBatch, GpuScfLinalg
 
 
 def nuclear_repulsion(basis: Basis) -> float:
@@ -59,7 +59,7 @@ def orthogonalizer(S: np.ndarray, smin: float = 1e-10) -> np.ndarray:
 class _RHFState:
     """One molecule's closed-shell iteration (host side of rhf_scf_update)."""
 
-    def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float):
+    def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float, device_linalg: bool = False):
         if basis.nelec % 2 or basis.mult != 1:
             raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
         self.n = basis.norb
@@ -68,8 +68,10 @@ class _RHFState:
         self.X = orthogonalizer(self.S)
         self.enuc = nuclear_repulsion(basis)
         self.ndiis, self.conv = ndiis, conv
-        self.eps, C = self.diag(self.H)
-        self.P = C[:, :self.nocc] @ C[:, :self.nocc].T
+        # the step of rhf_scf_update after F (X^T F X, diagonalise, C, P) on the
+        # GPU (patgpu_scf_*) or on the host
+        self.linalg = GpuScfLinalg(self.X, self.nocc) if device_linalg else None
+        self.eps, C, self.P = self.diag_density(self.H)
         self.fs, self.es = [], []
         self.e_old = None
         self.converged = False
@@ -78,6 +80,14 @@ class _RHFState:
     def diag(self, F):
         e, V = np.linalg.eigh(self.X.T @ F @ self.X)
         return e, self.X @ V
+
+    def diag_density(self, F):
+        """Orbital energies, orbitals and the half density of the Fock matrix F."""
+        if self.linalg is not None:
+            e, C, Pp, _ = self.linalg.density(pack(F))
+            return e, C, unpack(Pp, self.n)
+        e, C = self.diag(F)
+        return e, C, C[:, :self.nocc] @ C[:, :self.nocc].T
 
     def packed_density(self):
         return pack(self.P)
@@ -106,8 +116,7 @@ class _RHFState:
                 F = sum(ci * Fi for ci, Fi in zip(c, self.fs))
             except np.linalg.LinAlgError:
                 pass
-        self.eps, C = self.diag(F)
-        P_new = C[:, :self.nocc] @ C[:, :self.nocc].T
+        self.eps, C, P_new = self.diag_density(F)
         dP = float(np.max(np.abs(P_new - self.P)))
         self.P = P_new
         if self.e_old is not None and abs(energy - self.e_old) < self.conv and \
@@ -120,11 +129,15 @@ class _RHFState:
         G = unpack(Gp, self.n)
         F = self.H + G
         energy = 2.0 * np.sum(self.P * self.H) + np.sum(self.P * G) + self.enuc
-        eps, C = self.diag(F)
         o = self.nocc
-        P = C[:, :o] @ C[:, :o].T
-        W = (C[:, :o] * eps[:o]) @ C[:, :o].T
-        return RHFResult(energy=float(energy), P=pack(P), W=pack(W), C=C, eps=eps, iterations=self.it,
+        if self.linalg is not None:
+            eps, C, Pp, Wp = self.linalg.density(pack(F))
+            self.linalg.close()
+        else:
+            eps, C = self.diag(F)
+            Pp = pack(C[:, :o] @ C[:, :o].T)
+            Wp = pack((C[:, :o] * eps[:o]) @ C[:, :o].T)
+        return RHFResult(energy=float(energy), P=Pp, W=Wp, C=C, eps=eps, iterations=self.it,
                          converged=self.converged, enuc=self.enuc)
 
 
@@ -166,13 +179,13 @@ class IncrementalFock:
 
 def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
         maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
-        tau_inc: float = 1e-14) -> RHFResult:
+        tau_inc: float = 1e-14, device_linalg: bool = False) -> RHFResult:
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
-    from a full build."""
+    from a full build.  device_linalg=True diagonalises on the GPU."""
     gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
     Sp, Hp = _setup(gb, dpm)
-    st = _RHFState(basis, Sp, Hp, ndiis, conv)
+    st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg)
     fock = IncrementalFock(gb, tau_inc) if incremental else None
     while st.it < maxit and not st.converged:
         Pp = st.packed_density()
