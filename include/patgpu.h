@@ -171,6 +171,11 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
 #define PATGPU_GRAD_ALL 7
 int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int parts, int with_dpm,
                         double *grad);
+/* The open-shell form: E = sum_s [tr(P_s H) + tr(P_s G_s)/2] + E_nuc with
+ * G_s = J[Pa+Pb] - K[P_s] (uhfscf.c:29-55), at converged spin densities
+ * PA, PB and W_s = sum_occ e_i c_i c_i^T per spin (all packed). */
+int patgpu_uhf_gradient(patgpu_handle h, const double *PA, const double *PB, const double *WA, const double *WB,
+                        int parts, int with_dpm, double *grad);
 
 /* The reference's ERI files from the GPU integrals: the record stream of
  * two_electron_ints (twoints.c:188-418) -- 16-byte ERINT records

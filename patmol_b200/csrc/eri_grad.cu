@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
     double *s_red = s_gam + NCART;                  // [9][TQ]
     const int n = args.n;
     const double *__restrict__ P = args.D0;
+    const double *__restrict__ PB = args.D1;   // set: open shell (P = alpha, PB = beta spin density)
 
     for (long long base = (long long)blockIdx.x * NTEAM; base < args.nquart;
          base += (long long)gridDim.x * NTEAM) {
@@ -202,9 +203,18 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
                 const int ci = __ldg(&dm.desc[c].z);
                 const int ia = ci & 15, ib = (ci >> 4) & 15, ic = (ci >> 8) & 15, id = ci >> 12;
                 const int i = fa + ia, j = fb + ib, k = fc + ic, l = fd + id;
-                const double g = 2.0 * __ldg(P + (size_t)i * n + j) * __ldg(P + (size_t)k * n + l) -
-                                 0.5 * (__ldg(P + (size_t)i * n + k) * __ldg(P + (size_t)j * n + l) +
-                                        __ldg(P + (size_t)i * n + l) * __ldg(P + (size_t)j * n + k));
+                const size_t ij = (size_t)i * n + j, kl = (size_t)k * n + l, ik = (size_t)i * n + k,
+                             jl = (size_t)j * n + l, il = (size_t)i * n + l, jk = (size_t)j * n + k;
+                double g;
+                if (!PB) {   // closed shell, half density P
+                    g = 2.0 * __ldg(P + ij) * __ldg(P + kl) -
+                        0.5 * (__ldg(P + ik) * __ldg(P + jl) + __ldg(P + il) * __ldg(P + jk));
+                } else {     // open shell, spin densities Pa = P and Pb
+                    const double tij = __ldg(P + ij) + __ldg(PB + ij), tkl = __ldg(P + kl) + __ldg(PB + kl);
+                    g = 0.5 * tij * tkl -
+                        0.25 * (__ldg(P + ik) * __ldg(P + jl) + __ldg(P + il) * __ldg(P + jk) +
+                                __ldg(PB + ik) * __ldg(PB + jl) + __ldg(PB + il) * __ldg(PB + jk));
+                }
                 s_gam[c] = deg * g * c_norm[dm.la][ia] * c_norm[dm.lb][ib] * c_norm[dm.lc][ic] * c_norm[dm.ld][id];
             }
         }

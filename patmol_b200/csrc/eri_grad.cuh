@@ -7,6 +7,9 @@
 // ordered indices, and over the unique shell quartets with the degeneracy
 // factor deg of the Fock kernels
 //     Gamma_ijkl = 2 P_ij P_kl - (P_ik P_jl + P_il P_jk) / 2 .
+// Open shell (spin densities Pa, Pb, the UHF energy of uhfscf.c:54-55 with
+// G_s = J[Pa+Pb] - K[P_s]): with Pt = Pa + Pb
+//     Gamma_ijkl = Pt_ij Pt_kl / 2 - sum_s (P_s,ik P_s,jl + P_s,il P_s,jk) / 4 .
 // Its derivative with respect to the centre A of the first bra shell uses,
 // per primitive of exponent alpha,
 //     d phi_a / dA_x = 2 alpha phi_{a+1x} - a_x phi_{a-1x},
@@ -26,7 +29,8 @@ struct GradArgs {
 };
 
 // Launch the gradient kernel for the class in g over the quartets described
-// by a (implicit or list mode, swap = 0; a.D0 = full n x n half density).
+// by a (implicit or list mode, swap = 0; a.D0 = full n x n half density, or
+// with a.D1 set the alpha and beta spin densities).
 cudaError_t launch_eri_grad(const EriArgs &a, const GradArgs &g, cudaStream_t stream, int num_sms);
 
 // Dynamic shared memory the class needs (bytes per block).

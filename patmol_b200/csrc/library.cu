@@ -931,15 +931,20 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
 }
 
 // Two-electron gradient part: packed half density P, grad[3 ncen] += .
-static int grad_2e(patgpu_basis *h, const double *P, double *grad)
+static int grad_2e(patgpu_basis *h, const double *P, const double *PB, double *grad)
 {
-    int rc = ensure_work(h, false);
+    int rc = ensure_work(h, PB != nullptr);
     if (rc) return rc;
     const size_t nn = (size_t)h->n * h->n, no2 = (size_t)h->n * (h->n + 1) / 2;
     cudaStream_t s = h->stream;
     PG_CUDA(cudaMemcpyAsync(h->d_Pk0.p, P, sizeof(double) * no2, cudaMemcpyHostToDevice, s));
     unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(h->d_Pk0.as<double>(), h->d_D0.as<double>(),
                                                                     h->n);
+    if (PB) {
+        PG_CUDA(cudaMemcpyAsync(h->d_Pk1.p, PB, sizeof(double) * no2, cudaMemcpyHostToDevice, s));
+        unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(h->d_Pk1.as<double>(),
+                                                                        h->d_D1.as<double>(), h->n);
+    }
     DBuf dg;
     const size_t ng = 3 * (size_t)h->ncen;
     PG_CUDA(dg.ensure(sizeof(double) * ng));
@@ -953,6 +958,7 @@ static int grad_2e(patgpu_basis *h, const double *P, double *grad)
         EriArgs a = h->lists ? list_args(h, w, MODE_RHF, 2)
                              : class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
         a.D0 = h->d_D0.as<double>();
+        a.D1 = PB ? h->d_D1.as<double>() : nullptr;
         ga.la = w.la;
         ga.lb = w.lb;
         ga.lc = w.lc;
@@ -1568,6 +1574,36 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
                        nullptr);
 }
 
+int patgpu_uhf_gradient(patgpu_handle h, const double *PA, const double *PB, const double *WA, const double *WB,
+                        int parts, int with_dpm, double *grad)
+{
+    if (!h || !PA || !PB || !grad || parts < 0 || parts > PATGPU_GRAD_ALL)
+        return fail(PATGPU_EINVAL, "patgpu_uhf_gradient: bad argument");
+    if ((parts & PATGPU_GRAD_1E) && (!WA || !WB)) return fail(PATGPU_EINVAL, "patgpu_uhf_gradient: the 1e part needs W");
+    const size_t ng = 3 * (size_t)h->ncen, no2 = (size_t)h->n * (h->n + 1) / 2;
+    std::fill(grad, grad + ng, 0.0);
+    if (parts & PATGPU_GRAD_2E) {
+        int rc = grad_2e(h, PA, PB, grad);
+        if (rc) return rc;
+    }
+    if (parts & PATGPU_GRAD_1E) {
+        // sum over spins of tr(P_s dH) - tr(W_s dS) = 2 tr(P dH) - 2 tr(W dS)
+        // with the closed-shell-like P = (Pa + Pb)/2 and W = (Wa + Wb)/2
+        std::vector<double> Ph(no2), Wh(no2), g1(ng, 0.0);
+        for (size_t k = 0; k < no2; ++k) {
+            Ph[k] = 0.5 * (PA[k] + PB[k]);
+            Wh[k] = 0.5 * (WA[k] + WB[k]);
+        }
+        int rc = run_onebody_grad(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
+                                  h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n,
+                                  Ph.data(), Wh.data(), with_dpm, g1.data(), h->stream);
+        if (rc) return rc;
+        for (size_t k = 0; k < ng; ++k) grad[k] += g1[k];
+    }
+    if (parts & PATGPU_GRAD_NUC) grad_nuc(h, grad);
+    return 0;
+}
+
 int patgpu_set_density_screening(patgpu_handle h, double tau_dens)
 {
     if (!h || !(tau_dens >= 0.0)) return fail(PATGPU_EINVAL, "bad density-screening threshold");
@@ -1591,7 +1627,7 @@ int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int p
     const size_t ng = 3 * (size_t)h->ncen;
     std::fill(grad, grad + ng, 0.0);
     if (parts & PATGPU_GRAD_2E) {
-        int rc = grad_2e(h, P, grad);
+        int rc = grad_2e(h, P, nullptr, grad);
         if (rc) return rc;
     }
     if (parts & PATGPU_GRAD_1E) {

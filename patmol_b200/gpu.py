@@ -70,6 +70,7 @@ def lib():
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_mixed_stats.argtypes = [H, lp]
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.patgpu_uhf_gradient.argtypes = [H, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp]
         L.patgpu_write_eri_files.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                              ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ip, ip]
         L.patgpu_scf_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ctypes.POINTER(H)]
@@ -220,6 +221,17 @@ class GpuBasis:
         g = np.zeros(3 * self.basis.ncen)
         _check(lib().patgpu_rhf_gradient(self.h, _p(P), Wp, int(parts), int(bool(with_dpm)), _p(g)),
                "patgpu_rhf_gradient")
+        return g.reshape(-1, 3)
+
+    def uhf_gradient(self, PA, PB, WA=None, WB=None, parts: int = 7, with_dpm: bool = False):
+        """Nuclear gradient (ncen x 3) of the UHF energy at the packed spin
+        densities and energy-weighted spin densities (patgpu_uhf_gradient)."""
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None for x in (PA, PB, WA, WB)]
+        null = ctypes.POINTER(ctypes.c_double)()
+        ptr = [(_p(x) if x is not None else null) for x in arrs]
+        g = np.zeros(3 * self.basis.ncen)
+        _check(lib().patgpu_uhf_gradient(self.h, ptr[0], ptr[1], ptr[2], ptr[3], int(parts), int(bool(with_dpm)),
+                                         _p(g)), "patgpu_uhf_gradient")
         return g.reshape(-1, 3)
 
     def write_eri_files(self, prefix: str, basename: str, start: int = 0, rank: int = 0, nproc: int = 1,

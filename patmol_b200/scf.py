@@ -226,6 +226,102 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
     return out
 
 
+@dataclass
+class UHFResult:
+    energy: float
+    PA: np.ndarray         # packed alpha density
+    PB: np.ndarray         # packed beta density
+    WA: np.ndarray         # packed energy-weighted alpha density
+    WB: np.ndarray
+    iterations: int
+    converged: bool
+    enuc: float
+
+
+def uhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
+        maxit: int = 150, schwarz_tau: float = 1e-14, ndiis: int = 8) -> UHFResult:
+    """Open-shell SCF: the iteration of uhf_scf_update (uhfscf.c:23-78) with
+    G_s = J[Pa+Pb] - K[P_s] from the GPU (uhf_form_gmatrix), occupations of
+    uhfscf.c:120-122 (n_b = (N - (2S+1) + 1)/2, n_a = N - n_b), energy
+    E = sum_s [tr(P_s H) + tr(P_s G_s)/2] + E_nuc (uhfscf.c:54-55,
+    scfaux.c:100-118), and DIIS over both spins' commutators."""
+    gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
+    Sp, Hp = _setup(gb, dpm)
+    n = basis.norb
+    nb = (basis.nelec - (basis.mult - 1)) // 2
+    na = basis.nelec - nb
+    S, H = unpack(Sp, n), unpack(Hp, n)
+    X = orthogonalizer(S)
+    enuc = nuclear_repulsion(basis)
+
+    def diag(F):
+        e, V = np.linalg.eigh(X.T @ F @ X)
+        return e, X @ V
+
+    e0, C0 = diag(H)
+    P = [C0[:, :na] @ C0[:, :na].T, C0[:, :nb] @ C0[:, :nb].T]
+    occ = (na, nb)
+    hist_f, hist_e = [], []
+    e_old, converged, it = None, False, 0
+    for it in range(1, maxit + 1):
+        GA, GB = gb.uhf_form_gmatrix(pack(P[0]), pack(P[1]))
+        G = [unpack(GA, n), unpack(GB, n)]
+        F = [H + G[0], H + G[1]]
+        energy = sum(np.sum(P[s] * H) + 0.5 * np.sum(P[s] * G[s]) for s in range(2)) + enuc
+        errs = [X.T @ (F[s] @ P[s] @ S - S @ P[s] @ F[s]) @ X for s in range(2)]
+        hist_f.append(F)
+        hist_e.append(errs)
+        hist_f, hist_e = hist_f[-ndiis:], hist_e[-ndiis:]
+        if len(hist_f) > 1:
+            m = len(hist_f)
+            B = -np.ones((m + 1, m + 1))
+            B[m, m] = 0.0
+            for i in range(m):
+                for j in range(m):
+                    B[i, j] = sum(np.sum(hist_e[i][s] * hist_e[j][s]) for s in range(2))
+            rhs = np.zeros(m + 1)
+            rhs[m] = -1.0
+            try:
+                c = np.linalg.solve(B, rhs)[:m]
+                F = [sum(ci * Fi[s] for ci, Fi in zip(c, hist_f)) for s in range(2)]
+            except np.linalg.LinAlgError:
+                pass
+        newP = []
+        for s in range(2):
+            e, C = diag(F[s])
+            newP.append(C[:, :occ[s]] @ C[:, :occ[s]].T)
+        dP = max(float(np.abs(newP[s] - P[s]).max()) for s in range(2))
+        P = newP
+        if e_old is not None and abs(energy - e_old) < conv and dP < 1e-8 and \
+                max(float(np.abs(x).max()) for x in errs) < 1e-9:
+            converged = True
+            break
+        e_old = energy
+    GA, GB = gb.uhf_form_gmatrix(pack(P[0]), pack(P[1]))
+    G = [unpack(GA, n), unpack(GB, n)]
+    energy = sum(np.sum(P[s] * H) + 0.5 * np.sum(P[s] * G[s]) for s in range(2)) + enuc
+    out_P, out_W = [], []
+    for s in range(2):
+        e, C = diag(H + G[s])
+        o = occ[s]
+        out_P.append(pack(C[:, :o] @ C[:, :o].T))
+        out_W.append(pack((C[:, :o] * e[:o]) @ C[:, :o].T))
+    if gpu is None:
+        gb.close()
+    return UHFResult(energy=float(energy), PA=out_P[0], PB=out_P[1], WA=out_W[0], WB=out_W[1], iterations=it,
+                     converged=converged, enuc=enuc)
+
+
+def uhf_gradient(basis: Basis, res: UHFResult, dpm: bool = False, gpu: GpuBasis | None = None,
+                 parts: int = GpuBasis.GRAD_ALL, schwarz_tau: float = 1e-14) -> np.ndarray:
+    """dE/dR (ncen x 3, Eh/bohr) of the converged open-shell energy."""
+    gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
+    g = gb.uhf_gradient(res.PA, res.PB, res.WA, res.WB, parts=parts, with_dpm=dpm)
+    if gpu is None:
+        gb.close()
+    return g
+
+
 def rhf_gradient(basis: Basis, res: RHFResult, dpm: bool = False, gpu: GpuBasis | None = None,
                  parts: int = GpuBasis.GRAD_ALL, schwarz_tau: float = 1e-14) -> np.ndarray:
     """dE/dR (ncen x 3, Eh/bohr) of the converged closed-shell energy."""

@@ -173,3 +173,41 @@ def test_scf_gradient_invariances():
     torque = np.cross(b.coords, g).sum(axis=0)
     assert np.abs(torque).max() < 1e-7, torque
     assert np.abs(g).max() > 1e-3
+
+
+def test_uhf_two_electron_part_vs_oracle():
+    """Open shell: E2 = sum_s tr(P_s G_s)/2 with G_s = J[Pa+Pb] - K[P_s]."""
+    b = small_water(f_on_o=True, nelec=9)
+    PA = seeded_density(b.norb, 31)
+    PB = seeded_density(b.norb, 32)
+    wts = packed_weights(b.norb)
+    g = gpu.GpuBasis(b).uhf_gradient(PA, PB, parts=gpu.GpuBasis.GRAD_2E)
+
+    def e2(bx):
+        GA, GB = patref.Oracle(bx).gmat(PA, PB)
+        return float(0.5 * np.sum(wts * (PA * GA + PB * GB)))
+
+    close(g, richardson(e2, b))
+
+
+@pytest.mark.parametrize("dpm", [False, True], ids=["doublet", "doublet_dpm"])
+def test_uhf_scf_gradient_vs_energy_differences(dpm):
+    """The water cation doublet (9 electrons), with and without DPM."""
+    b = small_water(f_on_o=False, nelec=9)
+    b.mult = 2
+    if dpm:
+        b = b.dpm_augmented([0.2, 0.4, 3.0])
+    res = scf.uhf(b, dpm=dpm)
+    assert res.converged
+    g = scf.uhf_gradient(b, res, dpm=dpm)
+    h = 1e-4
+
+    def energy(bx):
+        r = scf.uhf(bx, dpm=dpm)
+        assert r.converged
+        return r.energy
+
+    coords = [(0, 2), (1, 1), (2, 2)] + ([(b.skipcen, 2)] if dpm else [])
+    for c, d in coords:
+        fd = (energy(b.displaced(c, d, h)) - energy(b.displaced(c, d, -h))) / (2 * h)
+        assert abs(g[c, d] - fd) < 2e-6, (c, d, g[c, d], fd)
