@@ -90,7 +90,9 @@ const char *patgpu_error_message(void);
  * normalize_shell, shell.c:26-56).  Per centre charge and xyz (bohr).
  * skipcen is left out of V and carries the DPM potential.  schwarz_tau:
  * quartets with Q_ab Q_cd < tau are skipped (0 disables screening).
- * Builds pairs and Schwarz bounds on the current CUDA device. */
+ * Builds pairs and Schwarz bounds on the current CUDA device; every later
+ * call on the handle must run with that device current (PATGPU_ESTATE
+ * otherwise).  One process may drive several devices, one handle each. */
 int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off, const int *nst,
                         const int *prim_off, const double *alpha, const double *coef, int ncen,
                         const double *charge, const double *xyz, int skipcen, double schwarz_tau,

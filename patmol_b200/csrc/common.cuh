@@ -19,6 +19,18 @@ namespace pg {
 
 constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
+#ifdef __CUDACC__
+// One-time per-device set-up (kernel attributes, constant tables): true the
+// first time the current device asks through this mask (bit d for device d).
+inline bool first_on_device(unsigned long long *mask)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return true;
+    const unsigned long long bit = 1ull << (dev & 63);
+    return !(__atomic_fetch_or(mask, bit, __ATOMIC_ACQ_REL) & bit);
+}
+#endif
+
 // Cartesian exponents in the order of basis.c:294-308: lx descending, then
 // ly descending.  Packed as lx | ly << 4 | lz << 8 for l <= 3.
 struct CartTab {

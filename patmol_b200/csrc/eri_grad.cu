@@ -65,11 +65,15 @@ int cexp_host(int l, int k, int dir)
     return 0;
 }
 
+// one copy per device (the tables hold device addresses)
 const GradTables &grad_tables()
 {
-    static GradTables t;
-    static std::once_flag once;
-    std::call_once(once, [] {
+    static GradTables tabs[64];
+    static std::once_flag once[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    GradTables &t = tabs[dev & 63];
+    std::call_once(once[dev & 63], [&t] {
         std::vector<int4> desc;
         std::vector<int2> ent;
         auto nc = [](int l) { return (l + 1) * (l + 2) / 2; };
@@ -393,11 +397,15 @@ cudaError_t launch_eri_grad(const EriArgs &a, const GradArgs &g, cudaStream_t st
     d.ent = t.ent + t.eoff[g.la][g.lb][g.lc][g.ld];
     d.nvalid = t.nvalid[g.la][g.lb][g.lc][g.ld];
     const size_t smem = sizeof(double) * (size_t)d.team * d.nteam;
-    static size_t configured = 0;
-    if (smem > configured) {
+    // the largest size set so far, per device (the attribute is per device)
+    static size_t configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    size_t &conf = configured[dev & 63];
+    if (smem > conf) {
         cudaError_t e = cudaFuncSetAttribute(eri_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = smem;
+        conf = smem;
     }
     long long blocks = (a.nquart + d.nteam - 1) / d.nteam;
     const long long cap = (long long)num_sms * 8;

@@ -492,12 +492,11 @@ template <int LA, int LB, int LC, int LD, int NDEN, typename R = double>
 cudaError_t launch_one(const EriArgs &a, cudaStream_t stream, int num_sms)
 {
     using S = Shape<LA, LB, LC, LD, NDEN>;
-    static bool configured = false;
-    if (!configured) {
+    static unsigned long long configured = 0;   // per device: the attribute is per device
+    if (first_on_device(&configured)) {
         cudaError_t e = cudaFuncSetAttribute(eri_class_kernel<LA, LB, LC, LD, NDEN, R>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
-        configured = true;
     }
     long long blocks = (a.nquart + S::NTEAM - 1) / S::NTEAM;
     long long cap = (long long)num_sms * 32;

@@ -313,12 +313,11 @@ template <int LA, int LB, int LC, int LD, typename R>
 cudaError_t launch_smem(const EriArgs &a, cudaStream_t stream, int num_sms)
 {
     using S = SmemShape<LA, LB, LC, LD, R>;
-    static bool configured = false;
-    if (!configured) {
+    static unsigned long long configured = 0;   // per device: the attribute is per device
+    if (first_on_device(&configured)) {
         cudaError_t e = cudaFuncSetAttribute(eri_smem_kernel<LA, LB, LC, LD, R>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
-        configured = true;
     }
     long long blocks = (a.nquart + S::NTEAM - 1) / S::NTEAM;
     long long cap = (long long)num_sms * 16;

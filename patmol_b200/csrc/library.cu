@@ -73,9 +73,12 @@ static cudaError_t upload(DBuf &b, const std::vector<T> &v, cudaStream_t s)
 }
 
 // ------------------------------------------------------------------ tables
-static std::once_flag g_rys_once;
-static DBuf *g_rys_coef = nullptr;   // per process (one device per process)
-static int g_rys_status = 0;
+// Rys coefficients and constant tables, uploaded once per device (a process
+// may drive several GPUs, one handle per device)
+constexpr int kMaxDevices = 64;
+static std::mutex g_tab_lock;
+static DBuf *g_rys_coef[kMaxDevices] = {};
+static int g_tab_state[kMaxDevices] = {};   // 0 not yet, 1 uploaded, -1 failed
 
 static RysConst host_rys_const()
 {
@@ -93,15 +96,20 @@ static RysConst host_rys_const()
 
 static int init_tables()
 {
-    std::call_once(g_rys_once, [] {
-        g_rys_coef = new DBuf();
-        if (g_rys_coef->ensure(sizeof(double) * rys_ncoef) != cudaSuccess ||
-            cudaMemcpy(g_rys_coef->p, rys_coef_host, sizeof(double) * rys_ncoef, cudaMemcpyHostToDevice) !=
-                cudaSuccess ||
-            upload_rys_constants(host_rys_const()) != cudaSuccess || upload_onebody_constants() != cudaSuccess)
-            g_rys_status = -1;
-    });
-    if (g_rys_status) return fail(PATGPU_ECUDA, "uploading the Rys tables failed");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return fail(PATGPU_ENODEV, "no usable current CUDA device");
+    std::lock_guard<std::mutex> g(g_tab_lock);
+    if (g_tab_state[dev] == 0) {
+        auto *b = new DBuf();
+        const bool ok =
+            b->ensure(sizeof(double) * rys_ncoef) == cudaSuccess &&
+            cudaMemcpy(b->p, rys_coef_host, sizeof(double) * rys_ncoef, cudaMemcpyHostToDevice) == cudaSuccess &&
+            upload_rys_constants(host_rys_const()) == cudaSuccess && upload_onebody_constants() == cudaSuccess;
+        g_rys_coef[dev] = b;
+        g_tab_state[dev] = ok ? 1 : -1;
+    }
+    if (g_tab_state[dev] < 0) return fail(PATGPU_ECUDA, "uploading the Rys tables to device %d failed", dev);
     return 0;
 }
 
@@ -128,6 +136,7 @@ static int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
 struct patgpu_basis {
     // snapshot
     int nsh = 0, ncen = 0, n = 0, skipcen = 0;
+    int dev = 0;                     // the device the handle's buffers live on
     std::vector<int> l, cen, off, nst, poff;
     std::vector<double> al, co, q, xyz;
     double tau = 0.0;
@@ -188,7 +197,7 @@ struct patgpu_basis {
         a.pp.K = d_pp_K.as<double>();
         a.pp.cut = d_pp_cut.as<double>();
         a.n = n;
-        a.rys_coef = pg::g_rys_coef->as<double>();
+        a.rys_coef = pg::g_rys_coef[dev]->as<double>();
         a.prim_cut = 1e-15;
         a.err = d_err.as<int>();
         return a;
@@ -881,10 +890,22 @@ static int density_filter(patgpu_basis *h, bool two)
     return 0;
 }
 
+// Calls on a handle must run with the handle's device current: its buffers
+// and tables live there.
+static int check_device(const patgpu_basis *h)
+{
+    int d = -1;
+    cudaGetDevice(&d);
+    if (d != h->dev)
+        return fail(PATGPU_ESTATE, "handle built on device %d used with device %d current", h->dev, d);
+    return 0;
+}
+
 // Host-buffer Fock build shared by the RHF / UHF / JK entry points.
 static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *P1, double *G0, double *G1)
 {
     if (!h) return fail(PATGPU_EINVAL, "null handle");
+    if (int rc0 = check_device(h)) return rc0;
     const bool two = mode != MODE_RHF;
     int rc = ensure_work(h, two);
     if (rc) return rc;
@@ -933,6 +954,7 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
 // Two-electron gradient part: packed half density P, grad[3 ncen] += .
 static int grad_2e(patgpu_basis *h, const double *P, const double *PB, double *grad)
 {
+    if (int rc0 = check_device(h)) return rc0;
     int rc = ensure_work(h, PB != nullptr);
     if (rc) return rc;
     const size_t nn = (size_t)h->n * h->n, no2 = (size_t)h->n * (h->n + 1) / 2;
@@ -1053,6 +1075,7 @@ int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off
     h->xyz.assign(xyz, xyz + 3 * ncen);
     int dev = 0;
     cudaGetDevice(&dev);
+    h->dev = dev;
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
@@ -1087,6 +1110,7 @@ int patgpu_basis_destroy(patgpu_handle h)
 int patgpu_set_quartets(patgpu_handle h, int start_shell, int rank, int nranks)
 {
     if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(PATGPU_EINVAL, "bad partition");
+    if (int rc0 = check_device(h)) return rc0;
     h->start_shell = start_shell;
     h->rank = rank;
     h->nranks = nranks;
@@ -1115,6 +1139,7 @@ int patgpu_jk(patgpu_handle h, const double *P, double *J, double *K)
 int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, void *stream)
 {
     if (!h || !dP || !dA) return fail(PATGPU_EINVAL, "null argument");
+    if (int rc0 = check_device(h)) return rc0;
     int rc = ensure_work(h, false);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
@@ -1230,6 +1255,7 @@ int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double 
 int patgpu_eri_quartets(patgpu_handle h, int nq, const int *sh4, double *out)
 {
     if (!h || nq < 0 || (nq && (!sh4 || !out))) return fail(PATGPU_EINVAL, "bad arguments");
+    if (int rc0 = check_device(h)) return rc0;
     // (shell i, shell j) -> pair index
     std::vector<int> pidx((size_t)h->nsh * h->nsh, -1);
     for (int u = 0; u < h->npair; ++u) {
@@ -1474,6 +1500,7 @@ int patgpu_fp64_peak(double *tflops)
 int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
 {
     if (!h || !(tau_fp32 >= 0.0)) return fail(PATGPU_EINVAL, "bad mixed-precision threshold");
+    if (int rc0 = check_device(h)) return rc0;
     h->tau_mix = tau_fp32;
     h->nquart_fp32 = 0;
     if (tau_fp32 <= 0.0 || tau_fp32 <= h->tau) return h->lists ? build_lists(h) : 0;
@@ -1546,6 +1573,7 @@ int patgpu_last_timing(patgpu_handle h, double *ns, int *launches)
 int patgpu_oneints(patgpu_handle h, double *S, double *T, double *H)
 {
     if (!h || !S || !T || !H) return fail(PATGPU_EINVAL, "null argument");
+    if (int rc0 = check_device(h)) return rc0;
     return run_oneints(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
                        h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n, S, T, H,
                        nullptr, h->stream);
@@ -1645,6 +1673,7 @@ int patgpu_rhf_gradient(patgpu_handle h, const double *P, const double *W, int p
 int patgpu_dpm(patgpu_handle h, double *H)
 {
     if (!h || !H) return fail(PATGPU_EINVAL, "null argument");
+    if (int rc0 = check_device(h)) return rc0;
     return run_oneints(h->nsh, h->l.data(), h->cen.data(), h->off.data(), h->nst.data(), h->poff.data(),
                        h->al.data(), h->co.data(), h->ncen, h->q.data(), h->xyz.data(), h->skipcen, h->n, nullptr,
                        nullptr, nullptr, H, h->stream);
@@ -1753,8 +1782,10 @@ int patgpu_batch_create(int nmol, const patgpu_handle *mols, patgpu_batch *out)
 {
     if (!out || nmol < 1 || !mols) return fail(PATGPU_EINVAL, "patgpu_batch_create: bad argument");
     *out = nullptr;
-    for (int m = 0; m < nmol; ++m)
+    for (int m = 0; m < nmol; ++m) {
         if (!mols[m]) return fail(PATGPU_EINVAL, "patgpu_batch_create: molecule %d has no handle", m);
+        if (int rc0 = check_device(mols[m])) return rc0;
+    }
     auto *b = new patgpu_batch_s();
     b->mols.assign(mols, mols + nmol);
     b->dP.reset(new DBuf[nmol]);
