@@ -53,6 +53,7 @@ struct EriArgs {
     double *out;            // export buffer
     const long long *out_off;
     const double *rys_coef;
+    int single_prim;        // 1: every shell pair has one primitive pair
     double prim_cut;        // skip primitive quartets whose coefficient-free
                             // prefactor is below this (1e-15 = twoints.c:110)
     int *err;               // device error word (0 = ok)

@@ -222,15 +222,18 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
                 s_gam[c] = deg * g * c_norm[dm.la][ia] * c_norm[dm.lb][ib] * c_norm[dm.lc][ic] * c_norm[dm.ld][id];
             }
         }
-        if (lane == 0) s_np[team] = active ? npb * npk : 0;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int m = 0;
-            for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
-            s_maxp = m;
+        int maxp = 1;   // block-uniform; 1 without a reduction when every shell has one primitive
+        if (!args.single_prim) {
+            if (lane == 0) s_np[team] = active ? npb * npk : 0;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int m = 0;
+                for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
+                s_maxp = m;
+            }
+            __syncthreads();
+            maxp = s_maxp;
         }
-        __syncthreads();
-        const int maxp = s_maxp;
         double g[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) g[k] = 0.0;

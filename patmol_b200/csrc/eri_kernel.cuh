@@ -252,15 +252,21 @@ eri_class_kernel(const EriArgs args)
                 }
             }
         }
-        if (in_team && lane == 0) s_np[team] = active ? npb * npk : 0;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int m = 0;
-            for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
-            s_maxp = m;
+        // primitive-quartet count of the block (block-uniform for the barriers
+        // inside the loop); with one primitive per shell it is 1 without a
+        // block reduction
+        int maxp = 1;
+        if (!args.single_prim) {
+            if (in_team && lane == 0) s_np[team] = active ? npb * npk : 0;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int m = 0;
+                for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
+                s_maxp = m;
+            }
+            __syncthreads();
+            maxp = s_maxp;
         }
-        __syncthreads();
-        const int maxp = s_maxp;
 
         // integrals of every bra component for this lane's ket component
         R acc[NCH][CH];

@@ -126,15 +126,18 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
             cdx = args.pr.abx[v]; cdy = args.pr.aby[v]; cdz = args.pr.abz[v];
         }
         for (int c = lane; c < NCART; c += TQ) s_out[c] = R(0);
-        if (lane == 0) s_np[team] = npb * npk;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int m = 0;
-            for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
-            s_maxp = m;
+        int maxp = 1;   // block-uniform; 1 without a reduction when every shell has one primitive
+        if (!args.single_prim) {
+            if (lane == 0) s_np[team] = npb * npk;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int m = 0;
+                for (int t = 0; t < NTEAM; ++t) m = max(m, s_np[t]);
+                s_maxp = m;
+            }
+            __syncthreads();
+            maxp = s_maxp;
         }
-        __syncthreads();
-        const int maxp = s_maxp;
 
         for (int ip = 0; ip < maxp; ++ip) {
             bool work = active && ip < npb * npk;

@@ -161,6 +161,7 @@ struct patgpu_basis {
     long long nquart = 0, nquart_unscreened = 0;
     pg::DBuf d_list;                 // compacted class quartet indices (uint64), when lists are on
     bool lists = false;
+    bool single_prim = false;        // every shell pair has exactly one primitive pair
     // density-weighted screening of host-buffer builds (tau_dens > 0): the
     // lists are filtered by Q_ab Q_cd max|D| against the build's density
     double tau_dens = 0.0;
@@ -199,6 +200,7 @@ struct patgpu_basis {
         a.n = n;
         a.rys_coef = pg::g_rys_coef[dev]->as<double>();
         a.prim_cut = 1e-15;
+        a.single_prim = single_prim ? 1 : 0;
         a.err = d_err.as<int>();
         return a;
     }
@@ -261,6 +263,8 @@ static int build_pairs(patgpu_basis *h)
             }
         h->pnum.push_back(np);
     }
+    h->single_prim = true;
+    for (int np : h->pnum) h->single_prim = h->single_prim && np == 1;
     cudaStream_t s = h->stream;
     cudaError_t e = cudaSuccess;
 #define UP(buf, vec) if (e == cudaSuccess) e = upload(h->buf, h->vec, s)
