@@ -490,7 +490,12 @@ eri_class_kernel(const EriArgs args)
                 }
             }
         }
-        __syncthreads();
+        // With more than one lane, the barrier before the cross-lane phase
+        // already separates every read of the staged densities from the next
+        // quartet's staging, and the next quartet writes the tables that
+        // phase reads only after its roots barrier.  A one-lane team's
+        // digestion reads the staged densities directly, so it keeps this one.
+        if constexpr (NCD == 1) __syncthreads();
     }
 }
 
