@@ -220,6 +220,8 @@ def batched_leg(a, torch, stream, nmol: int):
                         "config-0 s/p/d basis, RHF Fock build of every molecule per step",
             "molecules": nmol, "basis_functions": int(sum(bb.norb for bb in bases)), "quartets": q,
             "graph_nodes": st["graph_nodes"],
+            "l2": (f"not flushed: each step reads {8 * q / 1e9:.1f} GB of compacted quartet lists (8 B per "
+                   "quartet), far above the 126 MB L2"),
             "ms_per_step_graph": t_graph, "ms_per_step_sequential": t_seq,
             "quartets_per_s_graph": q / (t_graph * 1e-3), "speedup_graph_vs_sequential": t_seq / t_graph,
             "mixed": {"tau_fp32": a.tau_fp32, "fp32_quartets": stm["fp32_quartets"], "ms_per_step": t_mixed,
