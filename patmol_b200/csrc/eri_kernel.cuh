@@ -102,9 +102,11 @@ struct Shape {
 };
 
 // 2-D recursion and binomial transfer for one root and one direction;
-// writes I[a][b][c][d] to tab[(c(LD+1)+d) * TAB + a(LB+1)+b].
+// writes I[a][b][c][d] to tab[(c(LD+1)+d) * TAB + a(LB+1)+b], for every c
+// or (csel >= 0, a constant after unrolling at the call) only c = csel.
 template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void vrr_hrr(R *__restrict__ tab, R g00, R B00, R B10, R B01, R C, R Cp, R ab, R cd)
+__device__ __forceinline__ void vrr_hrr(R *__restrict__ tab, R g00, R B00, R B10, R B01, R C, R Cp, R ab, R cd,
+                                        int csel = -1)
 {
     constexpr int L12 = LA + LB, L34 = LC + LD, TAB = (LA + 1) * (LB + 1);
     R G[L12 + 1][L34 + 1];
@@ -133,6 +135,7 @@ __device__ __forceinline__ void vrr_hrr(R *__restrict__ tab, R g00, R B00, R B10
     for (int c = 0; c <= LC; ++c)
 #pragma unroll
         for (int d = 0; d <= LD; ++d) {
+            if (csel >= 0 && c != csel) continue;
             // ket transfer for every bra index: H[i] = sum_k C(d,k) cd^k G[i][c+d-k]
             R H[L12 + 1];
 #pragma unroll
@@ -302,8 +305,13 @@ eri_class_kernel(const EriArgs args)
             __syncthreads();
             if (work) {
                 const double ppq = p + q;
-                for (int j = lane; j < 3 * NR; j += TQ) {
-                    const int dim = j / NR, r = j - dim * NR;
+                // one job per (direction, root); when the team has lanes to
+                // spare, one per (direction, root, ket x-index c) instead, each
+                // redoing the short 2-D recursion and transferring one c
+                constexpr int NSPLIT = (LC > 0 && 3 * NR * (LC + 1) <= TQ) ? LC + 1 : 1;
+                for (int j = lane; j < 3 * NR * NSPLIT; j += TQ) {
+                    const int cs = j / (3 * NR), jj = j - cs * (3 * NR);
+                    const int dim = jj / NR, r = jj - dim * NR;
                     const double x = s_rw[r], w = s_rw[NR + r];
                     const double f = x / ppq, B00 = 0.5 * f;
                     const double B10 = (0.5 - B00 * q) / p, B01 = (0.5 - B00 * p) / q;
@@ -312,9 +320,18 @@ eri_class_kernel(const EriArgs args)
                     const double pq = dim == 0 ? pqx : (dim == 1 ? pqy : pqz);
                     const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
                     const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                    vrr_hrr<LA, LB, LC, LD, R>(reinterpret_cast<R *>(s_tab) + (dim * NR + r) * TSZ,
-                                               R(dim == 2 ? w * sr : 1.0), R(B00), R(B10), R(B01),
-                                               R(pa - q * pq * f), R(qc + p * pq * f), R(ab), R(cd));
+                    R *tab = reinterpret_cast<R *>(s_tab) + (dim * NR + r) * TSZ;
+                    if constexpr (NSPLIT == 1) {
+                        vrr_hrr<LA, LB, LC, LD, R>(tab, R(dim == 2 ? w * sr : 1.0), R(B00), R(B10), R(B01),
+                                                   R(pa - q * pq * f), R(qc + p * pq * f), R(ab), R(cd));
+                    } else {
+#pragma unroll
+                        for (int c0 = 0; c0 < NSPLIT; ++c0)
+                            if (c0 == cs)
+                                vrr_hrr<LA, LB, LC, LD, R>(tab, R(dim == 2 ? w * sr : 1.0), R(B00), R(B10), R(B01),
+                                                           R(pa - q * pq * f), R(qc + p * pq * f), R(ab), R(cd),
+                                                           c0);
+                    }
                 }
             }
             __syncthreads();
