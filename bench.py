@@ -40,10 +40,10 @@ WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 function
 # workload, from one ncu capture of dram__bytes_read.sum and
 # dram__bytes_write.sum (cold caches per launch); the capture's command and
 # per-kernel figures are kept with the other ncu summaries under profiles/.
-STEP_DRAM_BYTES = 219.1e6
+STEP_DRAM_BYTES = 194.7e6
 STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 55 class kernels of one "
-                    "Fock build (91.2 MB read incl. 58 MB of compacted quartet lists, 127.9 MB write, mostly "
-                    "local-memory write-back of three f classes)")
+                    "Fock build (91.6 MB read incl. 58 MB of compacted quartet lists, 103.1 MB write, mostly "
+                    "local-memory write-back of f-heavy lane-kernel classes)")
 
 
 def parse():
