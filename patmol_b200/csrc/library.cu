@@ -1227,6 +1227,7 @@ extern "C" {
 int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double *dG, void *stream)
 {
     if (!h || !dP || !dG) return fail(PATGPU_EINVAL, "null argument");
+    if (int rc0 = check_device(h)) return rc0;
     if (h->n > kNoAllocMaxN)
         return fail(PATGPU_EINVAL,
                     "patgpu_rhf_gmatrix_device_noalloc: the basis has %d functions but its fixed scratch holds "
