@@ -147,6 +147,26 @@ def test_water_gmat_close_to_reference():
     assert np.abs(G - g["G"]).max() > 1e-7   # the defect is visible
 
 
+@pytest.mark.slow
+def test_water_uhf_gmat_close_to_reference():
+    """UHF G_A, G_B of the restatement against the reference's
+    uhf_form_gmatrix (scfaux.c:555-714) at the fixture's two seeded
+    densities: equal up to the same root2 defect as the RHF build.  The
+    restatement's own spin blocks must also reduce to its RHF build when
+    both spin densities are equal (G_A = J[2P] - K[P] = 2J[P] - K[P])."""
+    b = configs.water_spd()
+    g = golden("water_spd.npz")
+    PA, PB = seeded_density(b.norb, 11), seeded_density(b.norb, 12)
+    O = patref.Oracle(b)
+    GA, GB = O.gmat(PA, PB)
+    for mine, ref in ((GA, g["GA"]), (GB, g["GB"])):
+        assert np.abs(mine - ref).max() < 1e-4
+        assert np.abs(mine - ref).max() > 1e-7   # the defect is visible
+    GAA, GBB = O.gmat(PA, PA)
+    G = O.gmat(PA)
+    assert np.abs(GAA - G).max() < 1e-12 and np.abs(GBB - G).max() < 1e-12
+
+
 def test_enuc():
     b = configs.water_spd()
     assert abs(patref.Oracle(b).enuc() - 9.1948428866511875) < 1e-12
