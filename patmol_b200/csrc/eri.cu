@@ -55,13 +55,21 @@ cudaError_t upload_rys_constants(const RysConst &rc)
 
 #define PG_CLASS(la, lb, lc, ld)                                                                       \
     extern template cudaError_t launch_smem<la, lb, lc, ld, double>(const EriArgs &, cudaStream_t, int); \
-    extern template cudaError_t launch_smem<la, lb, lc, ld, float>(const EriArgs &, cudaStream_t, int);
+    extern template cudaError_t launch_smem<la, lb, lc, ld, float>(const EriArgs &, cudaStream_t, int);  \
+    extern template cudaError_t launch_smem_occ<la, lb, lc, ld>(const EriArgs &, cudaStream_t, int);
 #include "eri_classes.inc"
 #undef PG_CLASS
 
 bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 {
     if (variant == 0 || variant == 2 || variant == 3 || variant == 4) return true;
+    if (variant == 5) {
+#define PG_CLASS(la, lb, lc, ld) \
+        if (LA == la && LB == lb && LC == lc && LD == ld) return SmemShape<la, lb, lc, ld, double>::HAS_OCC;
+#include "eri_classes.inc"
+#undef PG_CLASS
+        return false;
+    }
 #define PG_REG(la, lb, lc, ld) \
     if (LA == la && LB == lb && LC == lc && LD == ld) return variant == 1;
 #include "eri_reg_classes.inc"
@@ -80,6 +88,17 @@ cudaError_t launch_eri_class(int LA, int LB, int LC, int LD, const EriArgs &a, c
         b.swap = 0;                                                                   \
         return variant == 2 ? launch_smem<la, lb, lc, ld, double>(b, stream, num_sms) \
                             : launch_smem<la, lb, lc, ld, float>(b, stream, num_sms); \
+    }
+#include "eri_classes.inc"
+#undef PG_CLASS
+        return cudaErrorInvalidValue;
+    }
+    if (variant == 5) {
+#define PG_CLASS(la, lb, lc, ld)                                      \
+    if (LA == la && LB == lb && LC == lc && LD == ld) {              \
+        EriArgs b = a;                                                 \
+        b.swap = 0;                                                    \
+        return launch_smem_occ<la, lb, lc, ld>(b, stream, num_sms);   \
     }
 #include "eri_classes.inc"
 #undef PG_CLASS

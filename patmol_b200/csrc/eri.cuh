@@ -65,7 +65,8 @@ struct EriArgs {
 // class); 1: the register-only kernel (eri_reg.cuh, the classes of
 // eri_reg_classes.inc); 2: the shared-memory team kernel (eri_smem.cuh,
 // every class); 3 and 4: the FP32 forms of 2 and 0 (mixed precision; 4
-// takes one density set and runs as 3 for UHF).
+// takes one density set and runs as 3 for UHF); 5: the occupancy-hinted
+// FP64 form of 2 (the classes whose shared memory leaves room for it).
 cudaError_t launch_eri_class(int la, int lb, int lc, int ld, const EriArgs &a, cudaStream_t stream,
                              int num_sms, int variant = 0);
 bool eri_has_variant(int la, int lb, int lc, int ld, int variant);

@@ -39,6 +39,14 @@ struct SmemShape {
     // bytes per team: roots and weights (FP64), tables and integrals (R)
     static constexpr int TEAM_BYTES = ((16 * NR + (int)sizeof(R) * (3 * NR * TSZ + NCART)) + 15) / 16 * 16;
     static constexpr size_t SMEM = (size_t)TEAM_BYTES * NTEAM;
+    // blocks an SM can hold by shared memory (228 KB an SM, 1 KB reserved a
+    // block), and the blocks per SM the occupancy-hinted form asks of the
+    // register allocator: up to 4 (16 warps, at most 128 registers a thread)
+    static constexpr int SMEM_BLOCKS = (int)((228 * 1024) / (SMEM + 1024));
+    static constexpr int OCC = SMEM_BLOCKS >= 4 ? 4 : SMEM_BLOCKS;
+    // the hinted form exists where it lowers the register cap below the 255
+    // of the plain form, i.e. where shared memory leaves room for 3+ blocks
+    static constexpr bool HAS_OCC = OCC >= 3;
 };
 
 // 2-D recursion (rys.c:2269-2293 in the reference) and binomial transfer
@@ -93,8 +101,11 @@ __device__ __forceinline__ void vrr_hrr_smem(R *__restrict__ tab, R g00, R B00, 
                 }
 }
 
-template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
+// MINB > 1: the occupancy-hinted form, whose register allocation is capped so
+// that MINB blocks of 128 threads fit an SM (the autotuner times it beside
+// the plain form, MINB = 1).
+template <int LA, int LB, int LC, int LD, typename R, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) eri_smem_kernel(const EriArgs args)
 {
     using S = SmemShape<LA, LB, LC, LD, R>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCART = S::NCART;
@@ -312,22 +323,39 @@ __global__ void __launch_bounds__(128) eri_smem_kernel(const EriArgs args)
     }
 }
 
-template <int LA, int LB, int LC, int LD, typename R>
+template <int LA, int LB, int LC, int LD, typename R, int MINB = 1>
 cudaError_t launch_smem(const EriArgs &a, cudaStream_t stream, int num_sms)
 {
     using S = SmemShape<LA, LB, LC, LD, R>;
     static unsigned long long configured = 0;   // per device: the attribute is per device
     if (first_on_device(&configured)) {
-        cudaError_t e = cudaFuncSetAttribute(eri_smem_kernel<LA, LB, LC, LD, R>,
+        cudaError_t e = cudaFuncSetAttribute(eri_smem_kernel<LA, LB, LC, LD, R, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+        // the hinted form needs the whole shared-memory carveout for its
+        // MINB blocks; left to itself the driver may size the carveout for fewer
+        if (e == cudaSuccess && MINB > 1)
+            e = cudaFuncSetAttribute(eri_smem_kernel<LA, LB, LC, LD, R, MINB>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
     }
     long long blocks = (a.nquart + S::NTEAM - 1) / S::NTEAM;
     long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
-    eri_smem_kernel<LA, LB, LC, LD, R><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
+    eri_smem_kernel<LA, LB, LC, LD, R, MINB><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);
     return cudaGetLastError();
+}
+
+// FP64 occupancy-hinted form of the class (kernel variant 5); classes without
+// one (HAS_OCC false) return cudaErrorInvalidValue and are never offered it.
+template <int LA, int LB, int LC, int LD>
+cudaError_t launch_smem_occ(const EriArgs &a, cudaStream_t stream, int num_sms)
+{
+    using S = SmemShape<LA, LB, LC, LD, double>;
+    if constexpr (S::HAS_OCC)
+        return launch_smem<LA, LB, LC, LD, double, S::OCC>(a, stream, num_sms);
+    else
+        return cudaErrorInvalidValue;
 }
 
 }  // namespace pg

@@ -599,11 +599,13 @@ static int build_quartets(patgpu_basis *h)
 
 // Kernel-variant autotuner: every class has the lane team kernel (0) and the
 // shared-memory team kernel (2); the small classes also have the
-// register-only kernel (1).  Each variant is timed on the first
-// kTuneItems work items of the class's own quartet space and the fastest
-// kept.  Runs once per quartet partition, on a zero density and the
-// handle's own accumulator (the results are discarded).
-// PATGPU_VARIANT=lane|reg|smem forces a choice where it exists.
+// register-only kernel (1), and the classes whose shared memory leaves room
+// for 3 or more blocks an SM the occupancy-hinted shared-memory kernel (5).
+// Each variant is timed on the first kTuneItems work items of the class's
+// own quartet space and the fastest kept.  Runs once per quartet partition,
+// on a zero density and the handle's own accumulator (the results are
+// discarded).  PATGPU_VARIANT=lane|reg|smem|smem_occ forces a choice where
+// it exists.
 static int ensure_work(patgpu_basis *h, bool two);
 
 constexpr long long kTuneItems = 1 << 18;
@@ -615,6 +617,7 @@ static int tune_variants(patgpu_basis *h)
     if (force && !strcmp(force, "lane")) forced = 0;
     if (force && !strcmp(force, "reg")) forced = 1;
     if (force && !strcmp(force, "smem")) forced = 2;
+    if (force && !strcmp(force, "smem_occ")) forced = 5;
     for (auto &w : h->work) w.variant = 0;
     if (h->work.empty()) return 0;
     if (forced >= 0) {
@@ -634,13 +637,14 @@ static int tune_variants(patgpu_basis *h)
     cudaEvent_t e0, e1;
     PG_CUDA(cudaEventCreate(&e0));
     PG_CUDA(cudaEventCreate(&e1));
+    const bool log = getenv("PATGPU_TUNE_LOG") != nullptr;   // per-class timings to stderr
     for (auto &w : h->work) {
         a = h->lists ? list_args(h, w, MODE_RHF, 0) : class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
         a.D0 = h->d_D0.as<double>();
         a.A0 = h->d_A0.as<double>();
         a.nquart = std::min(a.nquart, kTuneItems);
         float best = 1e30f;
-        for (int var = 0; var <= 2; ++var) {
+        for (int var : {0, 1, 2, 5}) {
             if (!eri_has_variant(w.la, w.lb, w.lc, w.ld, var)) continue;
             float ms = 0.f;
             for (int rep = 0; rep < 2; ++rep) {   // first launch warms up
@@ -650,11 +654,14 @@ static int tune_variants(patgpu_basis *h)
                 PG_CUDA(cudaEventSynchronize(e1));
                 PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             }
+            if (log) fprintf(stderr, "patgpu tune (%d%d|%d%d) %lld quartets: variant %d %.1f us\n", w.la, w.lb, w.lc,
+                             w.ld, a.nquart, var, 1e3 * ms);
             if (ms < best) {
                 best = ms;
                 w.variant = var;
             }
         }
+        if (log) fprintf(stderr, "patgpu tune (%d%d|%d%d): chose variant %d\n", w.la, w.lb, w.lc, w.ld, w.variant);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -1,5 +1,5 @@
 """Every kernel variant, forced for every class where it exists
-(PATGPU_VARIANT=lane|reg|smem), gives the oracle's G within 1e-11 on a
+(PATGPU_VARIANT=lane|reg|smem|smem_occ), gives the oracle's G within 1e-11 on a
 65-function water basis whose shells cover all 55 quartet classes up to
 (ff|ff); the autotuner's own choice is checked the same way."""
 
@@ -23,7 +23,7 @@ def water_ref():
     return b, P, patref.Oracle(b).gmat(P)
 
 
-@pytest.mark.parametrize("variant", ["lane", "reg", "smem", None])
+@pytest.mark.parametrize("variant", ["lane", "reg", "smem", "smem_occ", None])
 def test_variant_matches_oracle(water_ref, variant, monkeypatch):
     b, P, ref = water_ref
     if variant is None:
