@@ -261,10 +261,13 @@ int patgpu_batch_last_timing(patgpu_batch b, double *kernel_ns);
  * transfer and assembly, while roots, weights, prefactors and every J/K
  * product and sum stay FP64; their integrals are below tau_fp32 in size, so
  * the absolute error per integral is about 1e-7 tau_fp32.  0 turns it off
- * (the default).  patgpu_mixed_stats returns how many quartets of this
- * handle run in FP32.  The FP32 window runs over the handle's compacted
- * quartet lists; a handle without lists (not enough device memory, or
- * PATGPU_LISTS=0) stays FP64 and reports 0. */
+ * (the default).  Per quartet class the library times the FP32 kernels
+ * against the class's FP64 kernel on that window and keeps the fastest, so
+ * a class whose window is too small to repay FP32 stays FP64 (one launch).
+ * patgpu_mixed_stats returns how many quartets of this handle run in FP32.
+ * The FP32 window runs over the handle's compacted quartet lists; a handle
+ * without lists (not enough device memory, or PATGPU_LISTS=0) stays FP64 and
+ * reports 0. */
 int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32);
 int patgpu_mixed_stats(patgpu_handle h, long long *n_fp32);
 

@@ -118,7 +118,7 @@ struct ClassWork {
     int la, lb, lc, ld;
     long long offset, count;     // count: quartets this rank owns after screening
     int variant = 0;             // kernel variant chosen for this class (see tune_variants)
-    int variant32 = 3;           // FP32 kernel of the mixed-precision window (3 or 4, see tune_fp32)
+    int variant32 = 3;           // kernel of the mixed-precision window: FP32 (3, 4) or `variant` (see tune_fp32)
     int u0 = 0, nu = 0, v0 = 0, nv = 0, same = 0;   // bra and ket pair ranges
     long long total = 0;         // unscreened quartets of the class (all ranks)
     long long items = 0;         // work items of this rank: ceil((total - rank) / nranks)
@@ -415,7 +415,10 @@ static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const 
     const double lo = h->tau > 0.0 ? h->tau : -1.0;
     const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
     if (h->lists) {
-        EriArgs a = list_args(h, w, proto.mode, 0);
+        // a class whose FP32 window is kept on its FP64 kernel (tune_fp32)
+        // runs both windows, adjacent in its unfiltered list, as one launch
+        const bool fold = mixed && w.variant32 == w.variant && !h->filtered;
+        EriArgs a = list_args(h, w, proto.mode, fold ? 2 : 0);
         a.D0 = proto.D0;
         a.D1 = proto.D1;
         a.A0 = proto.A0;
@@ -424,7 +427,7 @@ static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const 
             cudaError_t e = launch_eri_class(w.la, w.lb, w.lc, w.ld, a, s, h->num_sms, w.variant);
             if (e != cudaSuccess) return e;
         }
-        if (!mixed) return cudaSuccess;
+        if (!mixed || fold) return cudaSuccess;
         a = list_args(h, w, proto.mode, 1);
         a.D0 = proto.D0;
         a.D1 = proto.D1;
@@ -668,10 +671,13 @@ static int tune_variants(patgpu_basis *h)
     return 0;
 }
 
-// FP32 variant per class for the mixed-precision window: the shared-memory
-// kernel (3) against the lane kernel (4), timed like tune_variants on the
-// first kTuneItems quartets of the window.  PATGPU_VARIANT32=smem|lane
-// forces one.
+// Kernel per class for the mixed-precision window: the FP32 shared-memory
+// kernel (3), the FP32 lane kernel (4) and the class's own FP64 kernel,
+// timed like tune_variants on the first kTuneItems quartets of the window.
+// The FP64 kernel keeps the window where FP32 arithmetic does not pay for
+// its extra launch (small windows); nquart_fp32 then counts only the
+// quartets that do run in FP32.  PATGPU_VARIANT32=smem|lane forces an FP32
+// kernel for every class.
 static int tune_fp32(patgpu_basis *h)
 {
     const char *force = getenv("PATGPU_VARIANT32");
@@ -698,7 +704,7 @@ static int tune_fp32(patgpu_basis *h)
         a.A0 = h->d_A0.as<double>();
         a.nquart = std::min(a.nquart, kTuneItems);
         float best = 1e30f;
-        for (int var = 3; var <= 4; ++var) {
+        for (int var : {3, 4, w.variant}) {
             float ms = 0.f;
             for (int rep = 0; rep < 2; ++rep) {
                 PG_CUDA(cudaEventRecord(e0, s));
@@ -715,6 +721,9 @@ static int tune_fp32(patgpu_basis *h)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    h->nquart_fp32 = 0;
+    for (const auto &w : h->work)
+        if (w.variant32 == 3 || w.variant32 == 4) h->nquart_fp32 += w.count - w.nhi;
     return 0;
 }
 
