@@ -43,7 +43,8 @@ WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 function
 STEP_DRAM_BYTES = 194.7e6
 STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 55 class kernels of one "
                     "Fock build (91.6 MB read incl. 58 MB of compacted quartet lists, 103.1 MB write, mostly "
-                    "local-memory write-back of f-heavy lane-kernel classes)")
+                    "local-memory write-back of f-heavy lane-kernel classes); captured before the "
+                    "occupancy-hinted shared-memory variant, which four f classes now use")
 
 
 def parse():
