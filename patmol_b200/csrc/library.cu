@@ -674,10 +674,11 @@ static int tune_variants(patgpu_basis *h)
 // Kernel per class for the mixed-precision window: the FP32 shared-memory
 // kernel (3), the FP32 lane kernel (4) and the class's own FP64 kernel,
 // timed like tune_variants on the first kTuneItems quartets of the window.
-// The FP64 kernel keeps the window where FP32 arithmetic does not pay for
-// its extra launch (small windows); nquart_fp32 then counts only the
-// quartets that do run in FP32.  PATGPU_VARIANT32=smem|lane forces an FP32
-// kernel for every class.
+// The FP64 kernel keeps the window where it times faster than both FP32
+// kernels (in practice small windows, where a launch's fixed cost outweighs
+// the FP32 gain); launch_work then runs both windows as one launch, and
+// nquart_fp32 counts only the quartets that do run in FP32.
+// PATGPU_VARIANT32=smem|lane forces an FP32 kernel for every class.
 static int tune_fp32(patgpu_basis *h)
 {
     const char *force = getenv("PATGPU_VARIANT32");
