@@ -179,12 +179,16 @@ class IncrementalFock:
 
 def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
         maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
-        tau_inc: float = 1e-14, device_linalg: bool = False) -> RHFResult:
+        tau_inc: float = 1e-14, device_linalg: bool = False, tau_fp32: float = 0.0) -> RHFResult:
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
-    from a full build.  device_linalg=True diagonalises on the GPU."""
+    from a full build.  device_linalg=True diagonalises on the GPU.
+    tau_fp32 > 0 runs quartets whose Schwarz bound is below it in FP32
+    (mixed precision) in every build."""
     gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
     Sp, Hp = _setup(gb, dpm)
+    if tau_fp32 > 0.0:
+        gb.set_mixed_precision(tau_fp32)
     st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg)
     fock = IncrementalFock(gb, tau_inc) if incremental else None
     while st.it < maxit and not st.converged:
@@ -192,6 +196,8 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
         st.step(fock(Pp) if fock else gb.rhf_form_gmatrix(Pp))
     res = st.finish(gb.rhf_form_gmatrix(st.packed_density()))
     res.quartets_computed = fock.computed if fock else None
+    if tau_fp32 > 0.0:
+        gb.set_mixed_precision(0.0)
     if gpu is None:
         gb.close()
     return res
