@@ -457,7 +457,10 @@ def main():
     P_host = torch.from_numpy(rng.normal(scale=0.05, size=no2)).pin_memory()
     G_host = torch.empty(no2, dtype=torch.float64).pin_memory()
     P = P_host.to(dev)
-    A = torch.empty(n * n, dtype=torch.float64, device=dev)
+    # accumulator: n*n pairs of int64 words with exact fixed-point accumulation
+    # (summed as integers across ranks), n*n doubles with FP64 atomics
+    det = G.accumulator_bytes() == 16 * n * n
+    A = torch.empty(G.accumulator_bytes() // 8, dtype=torch.int64 if det else torch.float64, device=dev)
     Gd = torch.empty(no2, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
 

@@ -67,6 +67,13 @@ void dpm_ints(double *hmat);
  * S, T and H = T + V (all centres but skip_center()). */
 void one_electron_ints(double *Smat, double *Tmat, double *Hmat);
 
+/* Replaces clean_ERIFS (erifs.h:28, erifs.c:68-81): frees the device state
+ * bound to e, then runs the host program's own file clean-up and frees e
+ * through clean_ERIFS_files, the reference's clean_ERIFS compiled under that
+ * name (-Dclean_ERIFS=clean_ERIFS_files on erifs.c).  A host without it
+ * keeps e allocated. */
+void clean_ERIFS(ERIFS *e);
+
 /* ------------------------------------------------------------- explicit */
 typedef struct patgpu_basis *patgpu_handle;
 
@@ -97,6 +104,13 @@ int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off
                         const int *prim_off, const double *alpha, const double *coef, int ncen,
                         const double *charge, const double *xyz, int skipcen, double schwarz_tau,
                         patgpu_handle *out);
+/* The same, owning from the start only the quartets patgpu_set_quartets
+ * would select (start_shell, rank, nranks): one quartet-list build and one
+ * tuning pass instead of two. */
+int patgpu_basis_create_quartets(int nshell, const int *l, const int *cen, const int *off, const int *nst,
+                                 const int *prim_off, const double *alpha, const double *coef, int ncen,
+                                 const double *charge, const double *xyz, int skipcen, double schwarz_tau,
+                                 int start_shell, int rank, int nranks, patgpu_handle *out);
 int patgpu_basis_destroy(patgpu_handle h);
 
 /* Which quartets this handle owns: those whose largest shell index is
@@ -111,13 +125,30 @@ int patgpu_uhf_gmatrix(patgpu_handle h, const double *PA, const double *PB, doub
 /* J[P] and K[P] separately (packed; accumulate). */
 int patgpu_jk(patgpu_handle h, const double *P, double *J, double *K);
 
+/* No counterpart in the reference (its G build is a serial, hence
+ * deterministic, scatter: scfaux.c:446-495).  on = 1 (the default; the
+ * environment variable PATGPU_DETERMINISTIC=0 changes the default for new
+ * handles): every J/K contribution is rounded once to a fixed-point grid of
+ * 2^-60 and summed with 64-bit integer adds, which are exact and
+ * order-independent, so G is bitwise identical from run to run and across
+ * any split of the quartets over GPUs.  The accumulator then holds n x n
+ * elements of 16 bytes (two 64-bit integers).  on = 0: FP64 atomic adds,
+ * n x n doubles, last bits depend on the order the GPU's threads add in. */
+int patgpu_set_deterministic(patgpu_handle h, int on);
+/* Bytes of the n x n accumulator that patgpu_rhf_accumulate_device fills:
+ * 16 n^2 with deterministic accumulation, 8 n^2 without. */
+int patgpu_accumulator_bytes(patgpu_handle h, size_t *bytes);
+
 /* Device-resident Fock build: dP and dG are device pointers to packed
  * triangles; dG is overwritten (not accumulated).  stream is the
  * cudaStream_t to enqueue on, used as given (NULL = the legacy default
  * stream).  Enqueues only; the caller synchronises. */
 int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, void *stream);
-/* Same, leaving the unsymmetrised n x n accumulator in dA (G = A + A^T),
- * for callers that reduce partial results across GPUs before finishing. */
+/* Same, leaving the unsymmetrised n x n accumulator in dA (G = A + A^T,
+ * patgpu_accumulator_bytes(h) bytes), for callers that reduce partial
+ * results across GPUs before finishing: sum the partials elementwise, as
+ * doubles without deterministic accumulation, as 64-bit integers (wrapping)
+ * with it, then call patgpu_finish_gmatrix_device on the sum. */
 int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, void *stream);
 int patgpu_finish_gmatrix_device(patgpu_handle h, const double *dA, double *dG, void *stream);
 
@@ -126,9 +157,10 @@ int patgpu_finish_gmatrix_device(patgpu_handle h, const double *dA, double *dG, 
  * memory once they are running: a solver embedded in a host program that
  * owns all device memory through its own pool, or code on a path where a
  * cudaMalloc would synchronise the device or fail.  Its two n x n working
- * matrices live in a fixed 4 MiB array compiled into the library (every
- * GPU that loads the library holds it until the process exits), so the
- * basis must have at most 512 functions; larger bases are rejected with
+ * matrices (the density, and the accumulator at up to 16 bytes an element)
+ * live in a fixed 6 MiB array compiled into the library (every GPU that
+ * loads the library holds it until the process exits), so the basis must
+ * have at most 512 functions; larger bases are rejected with
  * PATGPU_EINVAL.  The handle itself is built beforehand by
  * patgpu_basis_create, which does allocate.  The first call on a device
  * looks up the array's device address there, so make that first call before
@@ -231,6 +263,15 @@ int patgpu_scf_density_host(patgpu_scf s, const double *F, double *P, double *W,
  * off.  patgpu_last_computed: quartets computed by the last host-buffer build. */
 int patgpu_set_density_screening(patgpu_handle h, double tau_dens);
 int patgpu_last_computed(patgpu_handle h, long long *quartets);
+/* Density-weighted precision of density-screened builds (no counterpart in
+ * the reference): a quartet kept by the screening whose bound
+ * Q_ab Q_cd max|D| is below tau32 is computed in FP32 arithmetic with FP64
+ * roots, prefactors and J/K sums -- in a difference build G[P_n - P_(n-1)]
+ * the density factor makes most contributions small, so their FP32 error
+ * (about 1e-7 of the contribution) stays far below the screening
+ * threshold's scale.  0 (the default) turns it off.  The first non-zero
+ * value times the FP32 kernels per class. */
+int patgpu_set_density_precision(patgpu_handle h, double tau32);
 
 /* Batches (no counterpart in the reference, which runs one molecule per
  * process): many molecules advanced in lock step.  A batch holds the
@@ -250,6 +291,15 @@ int patgpu_batch_create(int nmol, const patgpu_handle *mols, patgpu_batch *out);
 int patgpu_batch_destroy(patgpu_batch b);
 int patgpu_batch_buffers(patgpu_batch b, int m, double **dP, double **dG);
 int patgpu_batch_set_mixed_precision(patgpu_batch b, double tau_fp32);
+/* Density screening (and density-weighted precision, tau32) of every
+ * molecule's build, for incremental SCF: tau_dens > 0 makes launches use a
+ * second graph holding each molecule's density filter ahead of its class
+ * launches (the filtered work counts stay on the device, so the graph
+ * replays whatever densities the buffers hold); 0 returns to the plain
+ * graph.  patgpu_batch_last_computed: quartets computed by the last launch
+ * (synchronises the batch's stream). */
+int patgpu_batch_set_density_screening(patgpu_batch b, double tau_dens, double tau32);
+int patgpu_batch_last_computed(patgpu_batch b, long long *quartets);
 int patgpu_batch_launch(patgpu_batch b, void *stream);
 int patgpu_batch_rhf_gmatrix(patgpu_batch b, const double *const *P, double *const *G);
 int patgpu_batch_stats(patgpu_batch b, long long *out4);

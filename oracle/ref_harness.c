@@ -214,11 +214,147 @@ static int scf_update(Scf *S, int *iteration, double *eold, double *enrg)
     return 0;
 }
 
+/* ---- DIIS driver (closed shell; REF_HARNESS_DIIS=1) ----------------------
+ * The reference's averaging/Anderson damping (scfaux.c:64-95) stalls on many
+ * random molecules.  This driver keeps every reference computation -- G from
+ * rhf_form_gmatrix over the reference's own ERI files, spack_trans /
+ * spack_diag / form_cmatrix / form_pmatrix, calc_energy -- and only replaces
+ * the damping by Pulay's DIIS on the commutator FPS - SPF (in the
+ * orthogonalised basis), so that the reference's SCF energy exists for
+ * them.  Converged when |dE| < 1e-11 and max|error| < 1e-8. */
+#define DIIS_MAX 8
+static void unpack_full(int n, const double *p, double *f)
+{
+    int i, j;
+    for (i = 0; i < n; ++i)
+        for (j = 0; j <= i; ++j) f[i * n + j] = f[j * n + i] = p[i * (i + 1) / 2 + j];
+}
+
+static void matmul(int n, const double *a, const double *b, double *c)
+{
+    int i, j, k;
+    memset(c, 0, sizeof(double) * n * n);
+    for (i = 0; i < n; ++i)
+        for (k = 0; k < n; ++k) {
+            double aik = a[i * n + k];
+            if (aik == 0.0) continue;
+            for (j = 0; j < n; ++j) c[i * n + j] += aik * b[k * n + j];
+        }
+}
+
+/* x^T a x with x = S->x (full) */
+static void orth_transform(int n, const double *x, const double *a, double *out, double *tmp)
+{
+    int i, j, k;
+    matmul(n, a, x, tmp);
+    memset(out, 0, sizeof(double) * n * n);
+    for (k = 0; k < n; ++k)
+        for (i = 0; i < n; ++i) {
+            double xki = x[k * n + i];
+            if (xki == 0.0) continue;
+            for (j = 0; j < n; ++j) out[i * n + j] += xki * tmp[k * n + j];
+        }
+}
+
+/* Gaussian elimination with partial pivoting, m <= DIIS_MAX + 1 */
+static int solve_small(int m, double *A, double *b)
+{
+    int i, j, k;
+    for (k = 0; k < m; ++k) {
+        int piv = k;
+        for (i = k + 1; i < m; ++i)
+            if (fabs(A[i * m + k]) > fabs(A[piv * m + k])) piv = i;
+        if (fabs(A[piv * m + k]) < 1e-300) return -1;
+        if (piv != k) {
+            double t;
+            for (j = 0; j < m; ++j) { t = A[k * m + j]; A[k * m + j] = A[piv * m + j]; A[piv * m + j] = t; }
+            t = b[k]; b[k] = b[piv]; b[piv] = t;
+        }
+        for (i = k + 1; i < m; ++i) {
+            double f = A[i * m + k] / A[k * m + k];
+            for (j = k; j < m; ++j) A[i * m + j] -= f * A[k * m + j];
+            b[i] -= f * b[k];
+        }
+    }
+    for (k = m - 1; k >= 0; --k) {
+        double s = b[k];
+        for (j = k + 1; j < m; ++j) s -= A[k * m + j] * b[j];
+        b[k] = s / A[k * m + k];
+    }
+    return 0;
+}
+
+static double scf_run_diis(Scf *S, int *iters)
+{
+    int n = S->n, no2 = S->no2, it, i, j, nh = 0, head = 0;
+    double *fh[DIIS_MAX], *eh[DIIS_MAX];
+    double *Pf = dalloc(n * n), *Ff = dalloc(n * n), *Sf = dalloc(n * n), *t1 = dalloc(n * n);
+    double *t2 = dalloc(n * n), *err = dalloc(n * n), *fx = dalloc(no2);
+    double eold = 0.0, enrg = 0.0, emax = 0.0;
+    for (i = 0; i < DIIS_MAX; ++i) { fh[i] = dalloc(no2); eh[i] = dalloc(n * n); }
+    unpack_full(n, S->s, Sf);
+    for (it = 1; it <= S->maxit; ++it) {
+        memset(S->ga, 0, sizeof(double) * no2);
+        rhf_form_gmatrix(S->mints, S->pa, S->ga);
+        enrg = 2.0 * calc_energy(n, S->pa, S->h, S->ga);
+        for (i = 0; i < no2; ++i) fx[i] = S->h[i] + S->ga[i];
+        /* error FPS - SPF in the orthogonalised basis */
+        unpack_full(n, fx, Ff);
+        unpack_full(n, S->pa, Pf);
+        matmul(n, Ff, Pf, t1);
+        matmul(n, t1, Sf, t2);
+        for (i = 0; i < n; ++i)
+            for (j = 0; j < n; ++j) t1[i * n + j] = t2[i * n + j] - t2[j * n + i];
+        orth_transform(n, S->x, t1, err, t2);
+        emax = 0.0;
+        for (i = 0; i < n * n; ++i) emax = fabs(err[i]) > emax ? fabs(err[i]) : emax;
+        if (it > 1 && fabs(enrg - eold) < 1e-11 && emax < 1e-8) break;
+        eold = enrg;
+        memcpy(fh[head], fx, sizeof(double) * no2);
+        memcpy(eh[head], err, sizeof(double) * n * n);
+        head = (head + 1) % DIIS_MAX;
+        if (nh < DIIS_MAX) ++nh;
+        if (nh > 1) {
+            double B[(DIIS_MAX + 1) * (DIIS_MAX + 1)], c[DIIS_MAX + 1];
+            int m = nh + 1, a, b2;
+            for (a = 0; a < nh; ++a)
+                for (b2 = 0; b2 < nh; ++b2) {
+                    double s = 0.0;
+                    for (i = 0; i < n * n; ++i) s += eh[a][i] * eh[b2][i];
+                    B[a * m + b2] = s;
+                }
+            for (a = 0; a < nh; ++a) { B[a * m + nh] = B[nh * m + a] = -1.0; c[a] = 0.0; }
+            B[nh * m + nh] = 0.0;
+            c[nh] = -1.0;
+            if (solve_small(m, B, c) == 0) {
+                for (i = 0; i < no2; ++i) {
+                    double s = 0.0;
+                    for (a = 0; a < nh; ++a) s += c[a] * fh[a][i];
+                    fx[i] = s;
+                }
+            }
+        }
+        /* rhfscf.c:36-47 on the extrapolated Fock matrix */
+        memcpy(S->fock, fx, sizeof(double) * no2);
+        spack_trans(n, S->fock, S->x, S->work);
+        spack_diag(n, S->fock, S->w, S->ev, S->work);
+        form_cmatrix(n, S->ca, S->x, S->w);
+        form_pmatrix(n, S->nocc_a, S->ca, S->pa);
+    }
+    *iters = it;
+    fprintf(stderr, "ref_harness: DIIS SCF %d iterations, max|FPS-SPF| %.3e\n", it, emax);
+    for (i = 0; i < DIIS_MAX; ++i) { free(fh[i]); free(eh[i]); }
+    free(Pf); free(Ff); free(Sf); free(t1); free(t2); free(err); free(fx);
+    return enrg;
+}
+
 /* rhfscf.c:74-118: returns the final electronic energy */
 static double scf_run(Scf *S, int *iters)
 {
     int it = 0, done = 0;
     double eold = 0.0, enrg = 0.0;
+    const char *diis = getenv("REF_HARNESS_DIIS");
+    if (diis && diis[0] == '1' && !S->uhf) return scf_run_diis(S, iters);
     scf_update(S, &it, &eold, &enrg);
     it = 0;
     while (!done && it < S->maxit) done = scf_update(S, &it, &eold, &enrg);

@@ -33,6 +33,8 @@ int number_of_centers() __attribute__((weak));
 int skip_center() __attribute__((weak));
 void fatalError(const char *message) __attribute__((weak));
 FILE *createERIFile(int rank, int file_no, const char *bname) __attribute__((weak));   // erifs.c:84-90
+// the host's own clean_ERIFS (erifs.c:68-81) compiled under this name
+void clean_ERIFS_files(ERIFS *e) __attribute__((weak));
 }
 
 namespace {
@@ -110,14 +112,21 @@ void select_device_once()
     }
 }
 
-patgpu_handle make_handle(const Snap &s, double tau)
+patgpu_handle make_handle(const Snap &s, double tau, int start, int rank, int nproc)
 {
     select_device_once();
     patgpu_handle h = nullptr;
-    if (patgpu_basis_create(s.nsh, s.l.data(), s.cen.data(), s.off.data(), s.nst.data(), s.poff.data(),
-                            s.al.data(), s.co.data(), s.ncen, s.q.data(), s.xyz.data(), s.skip, tau, &h))
+    if (patgpu_basis_create_quartets(s.nsh, s.l.data(), s.cen.data(), s.off.data(), s.nst.data(), s.poff.data(),
+                                     s.al.data(), s.co.data(), s.ncen, s.q.data(), s.xyz.data(), s.skip, tau, start,
+                                     rank, nproc, &h))
         die("building the basis on the GPU");
     return h;
+}
+
+bool verbose()
+{
+    const char *e = getenv("PATGPU_VERBOSE");
+    return e && !strcmp(e, "1");
 }
 
 double schwarz_tau()
@@ -140,11 +149,21 @@ void two_electron_ints(ERIFS *tfiles, int start)
         g_handles.erase(it);
     }
     Snap s = snapshot();
-    patgpu_handle h = make_handle(s, schwarz_tau());
     int rank = tfiles->rank, nproc = tfiles->nproc > 0 ? tfiles->nproc : 1;
-    if (patgpu_set_quartets(h, start, rank % nproc, nproc)) die("two_electron_ints");
-    g_handles[tfiles] = h;
     tfiles->nfiles = 0;   // integral-direct: no ERI files
+    // Every quartet of the set has a shell with index >= start.  When all
+    // those shells are component-less (the DPM shells that rhf_dpm_calculation
+    // passes at every positron position, rhfscf.c:237), the set is empty: bind
+    // no device state and leave G untouched, as the reference's empty XINTS
+    // files do.
+    bool any = false;
+    for (int i = start; i < s.nsh; ++i) any = any || s.nst[i] > 0;
+    if (!any) {
+        g_handles[tfiles] = nullptr;
+        return;
+    }
+    patgpu_handle h = make_handle(s, schwarz_tau(), start, rank % nproc, nproc);
+    g_handles[tfiles] = h;
     // PATGPU_ERI_FILES=1: also write the reference's ERI files, for a host
     // program whose own file-reading G build stays linked
     const char *ef = getenv("PATGPU_ERI_FILES");
@@ -166,7 +185,7 @@ void rhf_form_gmatrix(const ERIFS *tfiles, const double *Pmat, double *Gmat)
     std::lock_guard<std::mutex> g(g_lock);
     auto it = g_handles.find(tfiles);
     if (it == g_handles.end()) die("rhf_form_gmatrix before two_electron_ints");
-    if (patgpu_rhf_gmatrix(it->second, Pmat, Gmat)) die("rhf_form_gmatrix");
+    if (it->second && patgpu_rhf_gmatrix(it->second, Pmat, Gmat)) die("rhf_form_gmatrix");
 }
 
 void uhf_form_gmatrix(const ERIFS *tfiles, const double *PmatA, const double *PmatB, double *GmatA, double *GmatB)
@@ -174,7 +193,7 @@ void uhf_form_gmatrix(const ERIFS *tfiles, const double *PmatA, const double *Pm
     std::lock_guard<std::mutex> g(g_lock);
     auto it = g_handles.find(tfiles);
     if (it == g_handles.end()) die("uhf_form_gmatrix before two_electron_ints");
-    if (patgpu_uhf_gmatrix(it->second, PmatA, PmatB, GmatA, GmatB)) die("uhf_form_gmatrix");
+    if (it->second && patgpu_uhf_gmatrix(it->second, PmatA, PmatB, GmatA, GmatB)) die("uhf_form_gmatrix");
 }
 
 void dpm_ints(double *hmat)
@@ -195,10 +214,28 @@ void one_electron_ints(double *Smat, double *Tmat, double *Hmat)
         die("one_electron_ints");
 }
 
+void clean_ERIFS(ERIFS *e)
+{
+    if (!e) return;
+    size_t left = 0;
+    {
+        std::lock_guard<std::mutex> g(g_lock);
+        auto it = g_handles.find(e);
+        if (it != g_handles.end()) {
+            if (it->second) patgpu_basis_destroy(it->second);
+            g_handles.erase(it);
+        }
+        left = g_handles.size();
+    }
+    if (verbose()) fprintf(stderr, "patgpu: clean_ERIFS released the handle's device state, %zu bound\n", left);
+    if (clean_ERIFS_files) clean_ERIFS_files(e);
+}
+
 void patgpu_release_all(void)
 {
     std::lock_guard<std::mutex> g(g_lock);
-    for (auto &kv : g_handles) patgpu_basis_destroy(kv.second);
+    for (auto &kv : g_handles)
+        if (kv.second) patgpu_basis_destroy(kv.second);
     g_handles.clear();
 }
 

@@ -5,6 +5,7 @@
 #include "eri_kernel.cuh"
 #include "eri_reg.cuh"
 #include "eri_smem.cuh"
+#include "eri_warp.cuh"
 
 namespace pg {
 
@@ -60,8 +61,23 @@ cudaError_t upload_rys_constants(const RysConst &rc)
 #include "eri_classes.inc"
 #undef PG_CLASS
 
+#define PG_WARP(la, lb, lc, ld, sw)                                                                    \
+    extern template cudaError_t launch_warp<la, lb, lc, ld, 1, double>(const EriArgs &, cudaStream_t, int); \
+    extern template cudaError_t launch_warp<la, lb, lc, ld, 1, float>(const EriArgs &, cudaStream_t, int);
+#include "eri_warp_classes.inc"
+#undef PG_WARP
+
 bool eri_has_variant(int LA, int LB, int LC, int LD, int variant)
 {
+    if (variant == 6 || variant == 7) {
+#define PG_WARP(la, lb, lc, ld, sw)                                          \
+        if ((sw == 0 && LA == la && LB == lb && LC == lc && LD == ld) ||    \
+            (sw == 1 && LA == lc && LB == ld && LC == la && LD == lb))      \
+            return true;
+#include "eri_warp_classes.inc"
+#undef PG_WARP
+        return false;
+    }
     if (variant == 0 || variant == 2 || variant == 3 || variant == 4) return true;
     if (variant == 5) {
 #define PG_CLASS(la, lb, lc, ld) \
@@ -81,6 +97,24 @@ cudaError_t launch_eri_class(int LA, int LB, int LC, int LD, const EriArgs &a, c
                              int num_sms, int variant)
 {
     if (variant == 4 && a.mode == MODE_UHF) variant = 3;   // the FP32 lane kernel has one density set
+    if (variant == 6 || variant == 7) {
+        // the warp kernels take one density set, Fock modes only and one
+        // primitive pair per shell pair; elsewhere the lane kernel (FP64) or
+        // the shared-memory kernel (FP32) serves
+        if (a.mode != MODE_UHF && a.mode != MODE_EXPORT && a.single_prim) {
+#define PG_WARP(la, lb, lc, ld, sw)                                                             \
+    if ((sw == 0 && LA == la && LB == lb && LC == lc && LD == ld) ||                           \
+        (sw == 1 && LA == lc && LB == ld && LC == la && LD == lb)) {                           \
+        EriArgs b = a;                                                                          \
+        b.swap = sw;                                                                            \
+        return variant == 6 ? launch_warp<la, lb, lc, ld, 1, double>(b, stream, num_sms)      \
+                            : launch_warp<la, lb, lc, ld, 1, float>(b, stream, num_sms);      \
+    }
+#include "eri_warp_classes.inc"
+#undef PG_WARP
+        }
+        variant = variant == 6 ? 0 : 3;
+    }
     if (variant == 2 || variant == 3) {
 #define PG_CLASS(la, lb, lc, ld)                                                     \
     if (LA == la && LB == lb && LC == lc && LD == ld) {                             \

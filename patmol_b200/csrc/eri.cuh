@@ -57,6 +57,12 @@ struct EriArgs {
     double prim_cut;        // skip primitive quartets whose coefficient-free
                             // prefactor is below this (1e-15 = twoints.c:110)
     int *err;               // device error word (0 = ok)
+    int det;                // 1: A0/A1 are fixed-point accumulators (acc_add)
+    // device work count: with nq_dev set, the launch runs *nq_dev items (a
+    // count an earlier kernel on the stream wrote; nquart is then only the
+    // launch's upper bound), the last ones of [0, nquart) when from_end is set
+    const unsigned long long *nq_dev;
+    int from_end;
 };
 
 // Launch the kernel of class (la lb | lc ld) on `stream`.  Returns a CUDA
@@ -66,7 +72,10 @@ struct EriArgs {
 // eri_reg_classes.inc); 2: the shared-memory team kernel (eri_smem.cuh,
 // every class); 3 and 4: the FP32 forms of 2 and 0 (mixed precision; 4
 // takes one density set and runs as 3 for UHF); 5: the occupancy-hinted
-// FP64 form of 2 (the classes whose shared memory leaves room for it).
+// FP64 form of 2 (the classes whose shared memory leaves room for it);
+// 6 and 7: the warp-synchronous kernel (eri_warp.cuh) in FP64 and FP32, for
+// the classes of eri_warp_classes.inc on one-primitive handles (RHF and JK;
+// UHF, export and contracted handles run 0 and 3 instead).
 cudaError_t launch_eri_class(int la, int lb, int lc, int ld, const EriArgs &a, cudaStream_t stream,
                              int num_sms, int variant = 0);
 bool eri_has_variant(int la, int lb, int lc, int ld, int variant);
@@ -74,6 +83,63 @@ bool eri_has_variant(int la, int lb, int lc, int ld, int variant);
 cudaError_t upload_rys_constants(const RysConst &rc);
 
 #ifdef __CUDACC__
+// Fixed-point accumulation (det = 1).  Each element of the accumulator is a
+// signed fixed-point number with 60 fraction bits held in two 64-bit
+// counters: word 1 counts units of 2^-28, word 0 units of 2^-60 (each addend
+// of word 0 lies in [-2^31, 2^31], so 2^32 additions fit; both words add as
+// two's complement integers).  A contribution is rounded once to the 2^-60
+// grid and added with integer arithmetic, which is exact and associative:
+// the accumulated value, and G, do not depend on the order in which threads
+// add.  Rounding to integers uses the 1.5 * 2^52 shift (the sum's low
+// mantissa bits are the rounded integer).  Contributions must stay below
+// 2^23 in magnitude; a larger or non-finite one sets *err, and the
+// finishing step then writes NaN.  det = 0: a plain FP64 atomic add.
+constexpr double kFixHi = 268435456.0;            // 2^28
+constexpr double kFixLo = 4294967296.0;           // 2^32
+constexpr double kFixShift = 6755399441055744.0;  // 1.5 * 2^52
+__device__ __forceinline__ void acc_add(double *A, size_t idx, double v, int det, int *err)
+{
+    if (!det) {
+        atomicAdd(A + idx, v);
+        return;
+    }
+    if (!(fabs(v) < 8388608.0)) {      // 2^23, also NaN
+        if (err) atomicOr(err, 1);
+        return;
+    }
+    unsigned long long *U = reinterpret_cast<unsigned long long *>(A) + 2 * idx;
+    const double sc = v * kFixHi;                 // |sc| < 2^51
+    const double t = sc + kFixShift;
+    const long long hi = __double_as_longlong(t) - __double_as_longlong(kFixShift);
+    const double r = sc - (t - kFixShift);        // exact, |r| <= 1/2
+    const long long lo = __double_as_longlong(fma(r, kFixLo, kFixShift)) - __double_as_longlong(kFixShift);
+    atomicAdd(U, (unsigned long long)lo);
+    atomicAdd(U + 1, (unsigned long long)hi);
+}
+
+// Value of a fixed-point element (signed words lo, hi) as a double, rounded once.
+__device__ __forceinline__ double fix_value(long long lo, long long hi)
+{
+    const long long h = hi + (lo >> 32);          // arithmetic shift: floor(lo / 2^32)
+    return (double)h * (1.0 / kFixHi) + (double)(lo & 0xffffffffll) * (1.0 / (kFixHi * kFixLo));
+}
+
+// Sum of two fixed-point elements as a double, rounded once.
+__device__ __forceinline__ double fix_sum(const unsigned long long *x, const unsigned long long *y)
+{
+    return fix_value((long long)x[0] + (long long)y[0], (long long)x[1] + (long long)y[1]);
+}
+
+// Number of work items of a launch and the first one (see nq_dev).
+__device__ __forceinline__ long long eri_work_count(const EriArgs &a)
+{
+    return a.nq_dev ? (long long)*a.nq_dev : a.nquart;
+}
+__device__ __forceinline__ long long eri_work_first(const EriArgs &a, long long nq)
+{
+    return (a.nq_dev && a.from_end) ? a.nquart - nq : 0;
+}
+
 // Work item qi -> (bra pair u, ket pair v) in this kernel's orientation;
 // false when the item is screened out.
 __device__ __forceinline__ bool eri_quartet_at(const EriArgs &a, long long qi, int &u, int &v)

@@ -36,7 +36,9 @@
 //     Kacc(f1,f3) += deg v D(f2,f4)    Kacc(f2,f4) += deg v D(f1,f3)
 //     Kacc(f1,f4) += deg v D(f2,f3)    Kacc(f2,f3) += deg v D(f1,f4)
 // gives J = (Jacc + Jacc^T)/4 and K = (Kacc + Kacc^T)/8; every target adds
-// once per quartet into the n x n accumulator (L2 resident, FP64 atomics).
+// once per quartet into the n x n accumulator (L2 resident) through acc_add:
+// exact fixed-point integer adds (order-independent, so G is bitwise
+// reproducible) or, with det = 0, FP64 atomics.
 #pragma once
 #include "eri.cuh"
 
@@ -212,12 +214,12 @@ eri_class_kernel(const EriArgs args)
     const double nfk = c_norm[LC][ic] * c_norm[LD][id];
     const int mode = args.mode;
     const int n = args.n;
+    const long long nq = eri_work_count(args), q0 = eri_work_first(args, nq);
 
-    for (long long base = (long long)blockIdx.x * NTEAM; base < args.nquart;
-         base += (long long)gridDim.x * NTEAM) {
+    for (long long base = (long long)blockIdx.x * NTEAM; base < nq; base += (long long)gridDim.x * NTEAM) {
         const long long qi = base + team;
         int u = 0, v = 0, npb = 0, npk = 0, pb0 = 0, pk0 = 0;
-        const bool active = in_team && qi < args.nquart && eri_quartet_at(args, qi, u, v);
+        const bool active = in_team && qi < nq && eri_quartet_at(args, q0 + qi, u, v);
         double ax = 0, ay = 0, az = 0, abx = 0, aby = 0, abz = 0;
         double cx = 0, cy = 0, cz = 0, cdx = 0, cdy = 0, cdz = 0;
         int fa = 0, fb = 0, fc = 0, fd = 0;
@@ -415,8 +417,8 @@ eri_class_kernel(const EriArgs args)
             {
                 const double o = sJ * jcd * nfk;
                 const size_t idx = (size_t)(fc + ic) * n + fd + id;
-                atomicAdd(args.A0 + idx, o);
-                if (NDEN == 2) atomicAdd(args.A1 + idx, o);
+                acc_add(args.A0, idx, o, args.det, args.err);
+                if (NDEN == 2) acc_add(args.A1, idx, o, args.det, args.err);
             }
             if constexpr (NCD == 1) {
                 // a single ket component: J(ab) and the exchange targets are lane-local
@@ -429,8 +431,8 @@ eri_class_kernel(const EriArgs args)
                             const int ia = ab / NB, ib = ab % NB;
                             const double o = sJ * (double)acc[c][j] * Dcd * c_norm[LA][ia] * c_norm[LB][ib];
                             const size_t idx = (size_t)(fa + ia) * n + fb + ib;
-                            atomicAdd(args.A0 + idx, o);
-                            if (NDEN == 2) atomicAdd(args.A1 + idx, o);
+                            acc_add(args.A0, idx, o, args.det, args.err);
+                            if (NDEN == 2) acc_add(args.A1, idx, o, args.det, args.err);
                         }
                     }
 #pragma unroll
@@ -439,13 +441,13 @@ eri_class_kernel(const EriArgs args)
                     const double sg = mode == MODE_JK ? sK : -sK;
 #pragma unroll
                     for (int a = 0; a < NA; ++a) {
-                        atomicAdd(A + (size_t)(fa + a) * n + fc, sg * Pac[s][a] * c_norm[LA][a]);
-                        atomicAdd(A + (size_t)(fa + a) * n + fd, sg * Pad[s][a] * c_norm[LA][a]);
+                        acc_add(A, (size_t)(fa + a) * n + fc, sg * Pac[s][a] * c_norm[LA][a], args.det, args.err);
+                        acc_add(A, (size_t)(fa + a) * n + fd, sg * Pad[s][a] * c_norm[LA][a], args.det, args.err);
                     }
 #pragma unroll
                     for (int b = 0; b < NB; ++b) {
-                        atomicAdd(A + (size_t)(fb + b) * n + fc, sg * Pbc[s][b] * c_norm[LB][b]);
-                        atomicAdd(A + (size_t)(fb + b) * n + fd, sg * Pbd[s][b] * c_norm[LB][b]);
+                        acc_add(A, (size_t)(fb + b) * n + fc, sg * Pbc[s][b] * c_norm[LB][b], args.det, args.err);
+                        acc_add(A, (size_t)(fb + b) * n + fd, sg * Pbd[s][b] * c_norm[LB][b], args.det, args.err);
                     }
                 }
             } else {
@@ -473,8 +475,8 @@ eri_class_kernel(const EriArgs args)
                         for (int k = 0; k < NCD; ++k) s += s_w[t * NCD + k];
                         const double o = sJ * s * c_norm[LA][ia] * c_norm[LB][ib];
                         const size_t idx = (size_t)(fa + ia) * n + fb + ib;
-                        atomicAdd(args.A0 + idx, o);
-                        if (NDEN == 2) atomicAdd(args.A1 + idx, o);
+                        acc_add(args.A0, idx, o, args.det, args.err);
+                        if (NDEN == 2) acc_add(args.A1, idx, o, args.det, args.err);
                         continue;
                     }
                     int row, col, base2, stride, cnt, off, lr, lc2, ir, icl;
@@ -501,8 +503,8 @@ eri_class_kernel(const EriArgs args)
                     for (int s = 0; s < NDEN; ++s) {
                         double sum = 0.0;
                         for (int k = 0; k < cnt; ++k) sum += s_part[((size_t)s * NCD + base2 + k * stride) * PS + off];
-                        if (mode == MODE_JK) atomicAdd(args.A1 + idx, f * sum);
-                        else atomicAdd((s == 0 ? args.A0 : args.A1) + idx, -f * sum);
+                        if (mode == MODE_JK) acc_add(args.A1, idx, f * sum, args.det, args.err);
+                        else acc_add(s == 0 ? args.A0 : args.A1, idx, -f * sum, args.det, args.err);
                     }
                 }
             }

@@ -82,10 +82,11 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
     const double *__restrict__ D0 = args.D0;
     const double *__restrict__ D1 = args.D1;
 
-    for (long long qi = (long long)blockIdx.x * blockDim.x + threadIdx.x; qi < args.nquart;
+    const long long nq = eri_work_count(args), q0 = eri_work_first(args, nq);
+    for (long long qi = (long long)blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
          qi += (long long)gridDim.x * blockDim.x) {
         int u, v;
-        if (!eri_quartet_at(args, qi, u, v)) continue;
+        if (!eri_quartet_at(args, q0 + qi, u, v)) continue;
         const int npb = args.pr.pnum[u], npk = args.pr.pnum[v];
         const int pb0 = args.pr.pstart[u], pk0 = args.pr.pstart[v];
         const double ax = args.pr.ax[u], ay = args.pr.ay[u], az = args.pr.az[u];
@@ -174,8 +175,8 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 #pragma unroll
             for (int cd = 0; cd < NCD; ++cd) s = fma(I[ab * NCD + cd], dsum(fc + cd / ND, fd + cd % ND), s);
             const size_t o = (size_t)(fa + ab / NB) * n + fb + ab % NB;
-            atomicAdd(args.A0 + o, sJ * s);
-            if (NDEN == 2) atomicAdd(args.A1 + o, sJ * s);
+            acc_add(args.A0, o, sJ * s, args.det, args.err);
+            if (NDEN == 2) acc_add(args.A1, o, sJ * s, args.det, args.err);
         }
 #pragma unroll
         for (int cd = 0; cd < NCD; ++cd) {
@@ -183,8 +184,8 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 #pragma unroll
             for (int ab = 0; ab < NAB; ++ab) s = fma(I[ab * NCD + cd], dsum(fa + ab / NB, fb + ab % NB), s);
             const size_t o = (size_t)(fc + cd / ND) * n + fd + cd % ND;
-            atomicAdd(args.A0 + o, sJ * s);
-            if (NDEN == 2) atomicAdd(args.A1 + o, sJ * s);
+            acc_add(args.A0, o, sJ * s, args.det, args.err);
+            if (NDEN == 2) acc_add(args.A1, o, sJ * s, args.det, args.err);
         }
         // exchange: K(a,c) over (b,d), K(a,d) over (b,c), K(b,c) over (a,d), K(b,d) over (a,c)
 #pragma unroll
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 #pragma unroll
                         for (int d = 0; d < ND; ++d)
                             k = fma(I[(a * NB + b) * NCD + c * ND + d], __ldg(D + (size_t)(fb + b) * n + fd + d), k);
-                    atomicAdd(A + (size_t)(fa + a) * n + fc + c, sg * k);
+                    acc_add(A, (size_t)(fa + a) * n + fc + c, sg * k, args.det, args.err);
                 }
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 #pragma unroll
                         for (int c = 0; c < NC; ++c)
                             k = fma(I[(a * NB + b) * NCD + c * ND + d], __ldg(D + (size_t)(fb + b) * n + fc + c), k);
-                    atomicAdd(A + (size_t)(fa + a) * n + fd + d, sg * k);
+                    acc_add(A, (size_t)(fa + a) * n + fd + d, sg * k, args.det, args.err);
                 }
             }
 #pragma unroll
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 #pragma unroll
                         for (int d = 0; d < ND; ++d)
                             k = fma(I[(a * NB + b) * NCD + c * ND + d], __ldg(D + (size_t)(fa + a) * n + fd + d), k);
-                    atomicAdd(A + (size_t)(fb + b) * n + fc + c, sg * k);
+                    acc_add(A, (size_t)(fb + b) * n + fc + c, sg * k, args.det, args.err);
                 }
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 #pragma unroll
                         for (int c = 0; c < NC; ++c)
                             k = fma(I[(a * NB + b) * NCD + c * ND + d], __ldg(D + (size_t)(fa + a) * n + fc + c), k);
-                    atomicAdd(A + (size_t)(fb + b) * n + fd + d, sg * k);
+                    acc_add(A, (size_t)(fb + b) * n + fd + d, sg * k, args.det, args.err);
                 }
             }
         }

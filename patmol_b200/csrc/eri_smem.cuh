@@ -119,11 +119,11 @@ __global__ void __launch_bounds__(128, MINB) eri_smem_kernel(const EriArgs args)
     R *s_tab = reinterpret_cast<R *>(s_rw + 2 * NR);   // [3][TSZ][NR]
     R *s_out = s_tab + 3 * NR * TSZ;                   // [NCART]
 
-    for (long long base = (long long)blockIdx.x * NTEAM; base < args.nquart;
-         base += (long long)gridDim.x * NTEAM) {
+    const long long nq = eri_work_count(args), q0 = eri_work_first(args, nq);
+    for (long long base = (long long)blockIdx.x * NTEAM; base < nq; base += (long long)gridDim.x * NTEAM) {
         const long long qi = base + team;
         int u = 0, v = 0, npb = 0, npk = 0, pb0 = 0, pk0 = 0;
-        const bool active = qi < args.nquart && eri_quartet_at(args, qi, u, v);
+        const bool active = qi < nq && eri_quartet_at(args, q0 + qi, u, v);
         double ax = 0, ay = 0, az = 0, abx = 0, aby = 0, abz = 0;
         double cx = 0, cy = 0, cz = 0, cdx = 0, cdy = 0, cdz = 0;
         if (active) {
@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(128, MINB) eri_smem_kernel(const EriArgs args)
                                 }
                         }
                         s *= sJ;
-                        atomicAdd(args.A0 + (size_t)row * n + col, s);
-                        if (mode == MODE_UHF) atomicAdd(args.A1 + (size_t)row * n + col, s);
+                        acc_add(args.A0, (size_t)row * n + col, s, args.det, args.err);
+                        if (mode == MODE_UHF) acc_add(args.A1, (size_t)row * n + col, s, args.det, args.err);
                     } else {
                         // exchange: four index pairings
                         double s0 = 0.0, s1 = 0.0;
@@ -310,10 +310,10 @@ __global__ void __launch_bounds__(128, MINB) eri_smem_kernel(const EriArgs args)
                         }
                         const size_t o = (size_t)row * n + col;
                         if (mode == MODE_JK) {
-                            atomicAdd(args.A1 + o, sK * s0);
+                            acc_add(args.A1, o, sK * s0, args.det, args.err);
                         } else {
-                            atomicAdd(args.A0 + o, -sK * s0);
-                            if (two) atomicAdd(args.A1 + o, -sK * s1);
+                            acc_add(args.A0, o, -sK * s0, args.det, args.err);
+                            if (two) acc_add(args.A1, o, -sK * s1, args.det, args.err);
                         }
                     }
                 }

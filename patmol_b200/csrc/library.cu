@@ -8,9 +8,11 @@
 #include <cstdio>
 #include <cstdarg>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/patgpu.h"
@@ -141,6 +143,9 @@ struct patgpu_basis {
     std::vector<double> al, co, q, xyz;
     double tau = 0.0;
     double tau_mix = 0.0;            // > 0: quartets with bounds in [tau, tau_mix) run in FP32
+    // 1: J/K accumulate as exact fixed-point integers (acc_add), so G is
+    // bitwise reproducible; the accumulators then hold 16 bytes an element
+    int det = 1;
     long long nquart_fp32 = 0;
     int start_shell = 0, rank = 0, nranks = 1;
     int num_sms = 148;
@@ -165,8 +170,11 @@ struct patgpu_basis {
     // density-weighted screening of host-buffer builds (tau_dens > 0): the
     // lists are filtered by Q_ab Q_cd max|D| against the build's density
     double tau_dens = 0.0;
+    // > 0 with tau_dens: a kept quartet whose density-weighted bound is below
+    // this runs in FP32 (the contribution, not just the integral, is small)
+    double tau_dens32 = 0.0;
     pg::DBuf d_soff, d_snst, d_dsh, d_flist, d_fcnt;
-    std::vector<unsigned long long> fcnt;   // per class: filtered FP64-window, FP32-window counts
+    std::vector<unsigned long long> fcnt;   // per class: filtered FP64, FP32 sublist counts
     bool filtered = false;                  // the current build runs over d_flist
     long long last_computed = 0;            // quartets computed by the last host-buffer build
     // work buffers
@@ -202,6 +210,7 @@ struct patgpu_basis {
         a.prim_cut = 1e-15;
         a.single_prim = single_prim ? 1 : 0;
         a.err = d_err.as<int>();
+        a.det = det;
         return a;
     }
 };
@@ -398,10 +407,14 @@ static EriArgs class_args(const patgpu_basis *h, const ClassWork &w, int mode, d
 static EriArgs list_args(const patgpu_basis *h, const ClassWork &w, int mode, int window)
 {
     EriArgs a = class_args(h, w, mode, -1.0, INFINITY);
-    if (h->filtered && window != 2) {   // density-screened sublists of this build
-        const unsigned long long *l = h->d_flist.as<unsigned long long>() + w.loff;
-        a.klist = window == 1 ? l + w.nhi : l;
-        a.nquart = (long long)h->fcnt[2 * w.idx + window];
+    if (h->filtered && window != 2) {
+        // density-screened sublists of this build (density_filter): the FP64
+        // part from the start of the class's region, the FP32 part at its end;
+        // their lengths are read on the device
+        a.klist = h->d_flist.as<unsigned long long>() + w.loff;
+        a.nquart = w.count;
+        a.nq_dev = h->d_fcnt.as<unsigned long long>() + 2 * w.idx + window;
+        a.from_end = window == 1;
         return a;
     }
     const unsigned long long *l = h->d_list.as<unsigned long long>() + w.loff;
@@ -413,7 +426,7 @@ static EriArgs list_args(const patgpu_basis *h, const ClassWork &w, int mode, in
 static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const EriArgs &proto, cudaStream_t s)
 {
     const double lo = h->tau > 0.0 ? h->tau : -1.0;
-    const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
+    const bool mixed = (h->tau_mix > lo && h->tau_mix > 0.0) || (h->filtered && h->tau_dens32 > 0.0);
     if (h->lists) {
         // a class whose FP32 window is kept on its FP64 kernel (tune_fp32)
         // runs both windows, adjacent in its unfiltered list, as one launch
@@ -602,16 +615,49 @@ static int build_quartets(patgpu_basis *h)
 
 // Kernel-variant autotuner: every class has the lane team kernel (0) and the
 // shared-memory team kernel (2); the small classes also have the
-// register-only kernel (1), and the classes whose shared memory leaves room
-// for 3 or more blocks an SM the occupancy-hinted shared-memory kernel (5).
+// register-only kernel (1), the classes whose shared memory leaves room
+// for 3 or more blocks an SM the occupancy-hinted shared-memory kernel (5),
+// and, on one-primitive handles, every class with at most 32 components on
+// one side the warp-synchronous kernel (6).
 // Each variant is timed on the first kTuneItems work items of the class's
 // own quartet space and the fastest kept.  Runs once per quartet partition,
 // on a zero density and the handle's own accumulator (the results are
-// discarded).  PATGPU_VARIANT=lane|reg|smem|smem_occ forces a choice where
+// discarded).  PATGPU_VARIANT=lane|reg|smem|smem_occ|warp forces a choice where
 // it exists.
 static int ensure_work(patgpu_basis *h, bool two);
 
 constexpr long long kTuneItems = 1 << 18;
+
+// The tuner's choices are kept for the whole process, per device, class,
+// primitive structure (one primitive pair per shell pair or not) and size
+// (fewer or more than 8192 quartets): later handles reuse them instead of
+// timing again.  Besides saving the tuning of every molecule of a batch,
+// this makes the kernel, hence the bits of every quartet's contribution,
+// the same in every handle of a process, so that fixed-point builds agree
+// bitwise across quartet partitions.
+static std::mutex g_tune_lock;
+static std::map<std::tuple<int, int, int, int, int>, int> g_tune_cache;
+
+static std::tuple<int, int, int, int, int> tune_key(const patgpu_basis *h, const ClassWork &w, int kind)
+{
+    return std::make_tuple(h->dev, ((w.la * 4 + w.lb) * 4 + w.lc) * 4 + w.ld, h->single_prim ? 1 : 0,
+                           w.count >= 8192 ? 1 : 0, kind);
+}
+
+static bool tune_cached(const patgpu_basis *h, const ClassWork &w, int kind, int *variant)
+{
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    auto it = g_tune_cache.find(tune_key(h, w, kind));
+    if (it == g_tune_cache.end()) return false;
+    *variant = it->second;
+    return true;
+}
+
+static void tune_store(const patgpu_basis *h, const ClassWork &w, int kind, int variant)
+{
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    g_tune_cache[tune_key(h, w, kind)] = variant;
+}
 
 static int tune_variants(patgpu_basis *h)
 {
@@ -621,6 +667,7 @@ static int tune_variants(patgpu_basis *h)
     if (force && !strcmp(force, "reg")) forced = 1;
     if (force && !strcmp(force, "smem")) forced = 2;
     if (force && !strcmp(force, "smem_occ")) forced = 5;
+    if (force && !strcmp(force, "warp")) forced = h->single_prim ? 6 : -1;
     for (auto &w : h->work) w.variant = 0;
     if (h->work.empty()) return 0;
     if (forced >= 0) {
@@ -642,13 +689,21 @@ static int tune_variants(patgpu_basis *h)
     PG_CUDA(cudaEventCreate(&e1));
     const bool log = getenv("PATGPU_TUNE_LOG") != nullptr;   // per-class timings to stderr
     for (auto &w : h->work) {
+        int cached = 0;
+        if (tune_cached(h, w, 0, &cached)) {
+            w.variant = cached;
+            if (log) fprintf(stderr, "patgpu tune (%d%d|%d%d): variant %d (chosen before)\n", w.la, w.lb, w.lc,
+                             w.ld, cached);
+            continue;
+        }
         a = h->lists ? list_args(h, w, MODE_RHF, 0) : class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, INFINITY);
         a.D0 = h->d_D0.as<double>();
         a.A0 = h->d_A0.as<double>();
         a.nquart = std::min(a.nquart, kTuneItems);
         float best = 1e30f;
-        for (int var : {0, 1, 2, 5}) {
+        for (int var : {0, 1, 2, 5, 6}) {
             if (!eri_has_variant(w.la, w.lb, w.lc, w.ld, var)) continue;
+            if (var == 6 && !h->single_prim) continue;
             float ms = 0.f;
             for (int rep = 0; rep < 2; ++rep) {   // first launch warms up
                 PG_CUDA(cudaEventRecord(e0, s));
@@ -665,6 +720,7 @@ static int tune_variants(patgpu_basis *h)
             }
         }
         if (log) fprintf(stderr, "patgpu tune (%d%d|%d%d): chose variant %d\n", w.la, w.lb, w.lc, w.ld, w.variant);
+        tune_store(h, w, 0, w.variant);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -678,7 +734,7 @@ static int tune_variants(patgpu_basis *h)
 // kernels (in practice small windows, where a launch's fixed cost outweighs
 // the FP32 gain); launch_work then runs both windows as one launch, and
 // nquart_fp32 counts only the quartets that do run in FP32.
-// PATGPU_VARIANT32=smem|lane forces an FP32 kernel for every class.
+// PATGPU_VARIANT32=smem|lane|warp forces an FP32 kernel for every class.
 static int tune_fp32(patgpu_basis *h)
 {
     const char *force = getenv("PATGPU_VARIANT32");
@@ -688,7 +744,15 @@ static int tune_fp32(patgpu_basis *h)
         for (auto &w : h->work) w.variant32 = 4;
         return 0;
     }
-    if (h->work.empty() || h->tau_mix <= 0.0) return 0;
+    if (force && !strcmp(force, "warp")) {
+        for (auto &w : h->work)
+            if (h->single_prim && eri_has_variant(w.la, w.lb, w.lc, w.ld, 7)) w.variant32 = 7;
+        return 0;
+    }
+    // timed on the Schwarz FP32 window, or, when only the density-weighted
+    // window of difference builds is set, on the class's whole list
+    const bool schwarz_window = h->tau_mix > 0.0;
+    if (h->work.empty() || !h->lists || (!schwarz_window && h->tau_dens32 <= 0.0)) return 0;
     int rc = ensure_work(h, false);
     if (rc) return rc;
     const size_t nn = (size_t)h->n * h->n;
@@ -697,15 +761,20 @@ static int tune_fp32(patgpu_basis *h)
     cudaEvent_t e0, e1;
     PG_CUDA(cudaEventCreate(&e0));
     PG_CUDA(cudaEventCreate(&e1));
-    const double lo = h->tau > 0.0 ? h->tau : -1.0;
     for (auto &w : h->work) {
-        EriArgs a = h->lists ? list_args(h, w, MODE_RHF, 1) : class_args(h, w, MODE_RHF, lo, h->tau_mix);
+        EriArgs a = list_args(h, w, MODE_RHF, schwarz_window ? 1 : 2);
         if (a.nquart <= 0) continue;
+        int cached = 0;
+        if (tune_cached(h, w, schwarz_window ? 1 : 2, &cached)) {
+            w.variant32 = cached;
+            continue;
+        }
         a.D0 = h->d_D0.as<double>();
         a.A0 = h->d_A0.as<double>();
         a.nquart = std::min(a.nquart, kTuneItems);
         float best = 1e30f;
-        for (int var : {3, 4, w.variant}) {
+        for (int var : {3, 4, 7, w.variant}) {
+            if (var == 7 && !(h->single_prim && eri_has_variant(w.la, w.lb, w.lc, w.ld, 7))) continue;
             float ms = 0.f;
             for (int rep = 0; rep < 2; ++rep) {
                 PG_CUDA(cudaEventRecord(e0, s));
@@ -719,12 +788,13 @@ static int tune_fp32(patgpu_basis *h)
                 w.variant32 = var;
             }
         }
+        tune_store(h, w, schwarz_window ? 1 : 2, w.variant32);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     h->nquart_fp32 = 0;
     for (const auto &w : h->work)
-        if (w.variant32 == 3 || w.variant32 == 4) h->nquart_fp32 += w.count - w.nhi;
+        if (w.variant32 == 3 || w.variant32 == 4 || w.variant32 == 7) h->nquart_fp32 += w.count - w.nhi;
     return 0;
 }
 
@@ -740,10 +810,16 @@ __global__ void unpack_kernel(const double *__restrict__ pk, double *__restrict_
     }
 }
 
-// packed[ij] = A[i][j] + A[j][i] (j <= i)
-__global__ void finish_kernel(const double *__restrict__ A, double *__restrict__ pk, int n)
+// packed[ij] = A[i][j] + A[j][i] (j <= i).  det: A holds fixed-point
+// elements (two 64-bit words each, acc_add); the two are added exactly and
+// rounded once, and a set *err (an out-of-range or non-finite contribution)
+// gives NaN everywhere.
+__global__ void finish_kernel(const double *__restrict__ A, double *__restrict__ pk, int n, int det,
+                              const int *__restrict__ err)
 {
     long long no2 = (long long)n * (n + 1) / 2;
+    const bool bad = det && err && *err;
+    const unsigned long long *U = reinterpret_cast<const unsigned long long *>(A);
     for (long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x; ij < no2;
          ij += (long long)gridDim.x * blockDim.x) {
         // invert ij = i(i+1)/2 + j
@@ -751,7 +827,11 @@ __global__ void finish_kernel(const double *__restrict__ A, double *__restrict__
         while ((long long)(i + 1) * (i + 2) / 2 <= ij) ++i;
         while ((long long)i * (i + 1) / 2 > ij) --i;
         int j = (int)(ij - (long long)i * (i + 1) / 2);
-        pk[ij] = A[(size_t)i * n + j] + A[(size_t)j * n + i];
+        if (!det)
+            pk[ij] = A[(size_t)i * n + j] + A[(size_t)j * n + i];
+        else
+            pk[ij] = bad ? __longlong_as_double(0x7ff8000000000000ll)
+                         : fix_sum(U + 2 * ((size_t)i * n + j), U + 2 * ((size_t)j * n + i));
     }
 }
 
@@ -798,15 +878,37 @@ static int ensure_work(patgpu_basis *h, bool two)
 {
     const size_t nn = (size_t)h->n * h->n, no2 = (size_t)h->n * (h->n + 1) / 2;
     PG_CUDA(h->d_D0.ensure(sizeof(double) * nn));
-    PG_CUDA(h->d_A0.ensure(sizeof(double) * nn));
+    PG_CUDA(h->d_A0.ensure(2 * sizeof(double) * nn));   // room for fixed-point elements
     PG_CUDA(h->d_Pk0.ensure(sizeof(double) * no2));
     PG_CUDA(h->d_Gk0.ensure(sizeof(double) * no2));
     if (two) {
         PG_CUDA(h->d_D1.ensure(sizeof(double) * nn));
-        PG_CUDA(h->d_A1.ensure(sizeof(double) * nn));
+        PG_CUDA(h->d_A1.ensure(2 * sizeof(double) * nn));
         PG_CUDA(h->d_Pk1.ensure(sizeof(double) * no2));
         PG_CUDA(h->d_Gk1.ensure(sizeof(double) * no2));
     }
+    return 0;
+}
+
+// Bytes of one n x n accumulator in the handle's accumulation mode.
+static size_t acc_bytes(const patgpu_basis *h)
+{
+    return (h->det ? 2 : 1) * sizeof(double) * (size_t)h->n * h->n;
+}
+
+// Zero an accumulator (and the handle's device error word) on stream s.
+static int acc_clear(const patgpu_basis *h, void *A, cudaStream_t s)
+{
+    PG_CUDA(cudaMemsetAsync(A, 0, acc_bytes(h), s));
+    PG_CUDA(cudaMemsetAsync(h->d_err.p, 0, sizeof(int), s));
+    return 0;
+}
+
+static int finish(const patgpu_basis *h, const double *A, double *G, cudaStream_t s)
+{
+    const long long no2 = (long long)h->n * (h->n + 1) / 2;
+    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(A, G, h->n, h->det, h->d_err.as<int>());
+    PG_CUDA(cudaGetLastError());
     return 0;
 }
 
@@ -837,56 +939,66 @@ __global__ void shell_dmax_kernel(const double *__restrict__ D0, const double *_
     }
 }
 
+// Append the lanes with keep set to out[*cnt ...] (forward) or, with
+// backward, to out[-1 - *cnt ...] (growing down from out), with one
+// warp-aggregated atomic.
+__device__ __forceinline__ void warp_append(bool keep, unsigned long long v, unsigned long long *out,
+                                            unsigned long long *cnt, bool backward)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == lead) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, lead);
+    const unsigned long long k = base + __popc(m & ((1u << lane) - 1u));
+    if (keep) {
+        if (backward) *(out - 1 - (long long)k) = v;
+        else out[k] = v;
+    }
+}
+
 // Keep the list entries whose contribution bound Q_ab Q_cd max(4|D_ab|,
 // 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|) reaches tau (shell-block maxima;
-// the factor 4 covers the Coulomb weight), appended with warp-aggregated
-// atomics.
+// the factor 4 covers the Coulomb weight).  A kept entry goes to the FP32
+// sublist (written downward from end32) when all32 is set (the Schwarz FP32
+// window) or its bound is below tau32, else to the FP64 sublist (upward from
+// out64); counts in cnt[0] and cnt[1].
 __global__ void density_filter_kernel(const EriArgs a, const double *__restrict__ dsh, int nsh, double tau,
-                                      unsigned long long *out, unsigned long long *cnt)
+                                      double tau32, int all32, unsigned long long *out64,
+                                      unsigned long long *end32, unsigned long long *cnt)
 {
     for (long long qi0 = (long long)blockIdx.x * blockDim.x; qi0 < a.nquart;
          qi0 += (long long)gridDim.x * blockDim.x) {
         const long long qi = qi0 + threadIdx.x;
         int u = 0, v = 0;
         bool keep = qi < a.nquart && eri_quartet_at(a, qi, u, v);
+        bool low = false;
         if (keep) {
             const int sa = a.pr.sa[u], sb = a.pr.sb[u], sc = a.pr.sa[v], sd = a.pr.sb[v];
             const double dj = 4.0 * fmax(dsh[sa * nsh + sb], dsh[sc * nsh + sd]);
             const double dk = fmax(fmax(dsh[sa * nsh + sc], dsh[sa * nsh + sd]), fmax(dsh[sb * nsh + sc], dsh[sb * nsh + sd]));
-            keep = a.Q[u] * a.Q[v] * fmax(dj, dk) >= tau;
+            const double bound = a.Q[u] * a.Q[v] * fmax(dj, dk);
+            keep = bound >= tau;
+            low = all32 || bound < tau32;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (!m) continue;
-        const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
-        unsigned long long base = 0;
-        if (lane == lead) base = atomicAdd(cnt, (unsigned long long)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, lead);
-        if (keep) out[base + __popc(m & ((1u << lane) - 1u))] = a.klist[qi];
+        const unsigned long long k = qi < a.nquart ? a.klist[qi] : 0ull;
+        warp_append(keep && !low, k, out64, cnt, false);
+        warp_append(keep && low, k, end32, cnt + 1, true);
     }
 }
 
 // Filter every class's list(s) against the density of this build (d_D0, and
-// d_D1 for UHF) into d_flist; host_fock then launches over the sublists.
-static int density_filter(patgpu_basis *h, bool two)
+// d_D1 for UHF) into d_flist, enqueued on s: the counts stay on the device
+// (the class launches read them there), so a build with the filter can be
+// captured in a CUDA graph.
+static int density_filter_enqueue(patgpu_basis *h, bool two, cudaStream_t s)
 {
-    cudaStream_t s = h->stream;
-    if (!h->d_soff.p) {
-        std::vector<int> soff(h->nsh), snst(h->nsh);
-        for (int i = 0; i < h->nsh; ++i) {
-            soff[i] = h->off[i];
-            snst[i] = h->nst[i];
-        }
-        PG_CUDA(upload(h->d_soff, soff, s));
-        PG_CUDA(upload(h->d_snst, snst, s));
-    }
     const int nsh = h->nsh;
-    PG_CUDA(h->d_dsh.ensure(sizeof(double) * (size_t)nsh * nsh));
     shell_dmax_kernel<<<grid_for((long long)nsh * nsh, h->num_sms), 256, 0, s>>>(
         h->d_D0.as<double>(), two ? h->d_D1.as<double>() : nullptr, h->n, h->d_soff.as<int>(), h->d_snst.as<int>(),
         nsh, h->d_dsh.as<double>());
-    PG_CUDA(h->d_flist.ensure(std::max<size_t>(h->d_list.bytes, 16)));
     const size_t nc = 2 * std::max<size_t>(h->work.size(), 1);
-    PG_CUDA(h->d_fcnt.ensure(sizeof(unsigned long long) * nc));
     PG_CUDA(cudaMemsetAsync(h->d_fcnt.p, 0, sizeof(unsigned long long) * nc, s));
     const double lo = h->tau > 0.0 ? h->tau : -1.0;
     const bool mixed = h->tau_mix > lo && h->tau_mix > 0.0;
@@ -896,18 +1008,30 @@ static int density_filter(patgpu_basis *h, bool two)
             EriArgs a = list_args(h, w, MODE_RHF, win);
             if (a.nquart <= 0) continue;
             const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
-            density_filter_kernel<<<std::max(g, 1), 256, 0, s>>>(a, h->d_dsh.as<double>(), nsh, h->tau_dens,
-                                                                  out + w.loff + (win ? w.nhi : 0),
-                                                                  h->d_fcnt.as<unsigned long long>() + 2 * w.idx + win);
+            density_filter_kernel<<<std::max(g, 1), 256, 0, s>>>(
+                a, h->d_dsh.as<double>(), nsh, h->tau_dens, h->tau_dens32, win, out + w.loff,
+                out + w.loff + w.count, h->d_fcnt.as<unsigned long long>() + 2 * w.idx);
         }
     PG_CUDA(cudaGetLastError());
-    h->fcnt.assign(nc, 0);
-    PG_CUDA(cudaMemcpyAsync(h->fcnt.data(), h->d_fcnt.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, s));
-    PG_CUDA(cudaStreamSynchronize(s));
-    h->filtered = true;
-    long long tot = 0;
-    for (auto c : h->fcnt) tot += (long long)c;
-    h->last_computed = tot;
+    return 0;
+}
+
+// Device buffers of the density filter (shell offsets, block maxima, the
+// filtered list and its counts).
+static int density_filter_buffers(patgpu_basis *h)
+{
+    if (!h->d_soff.p) {
+        std::vector<int> soff(h->nsh), snst(h->nsh);
+        for (int i = 0; i < h->nsh; ++i) {
+            soff[i] = h->off[i];
+            snst[i] = h->nst[i];
+        }
+        PG_CUDA(upload(h->d_soff, soff, h->stream));
+        PG_CUDA(upload(h->d_snst, snst, h->stream));
+    }
+    PG_CUDA(h->d_dsh.ensure(sizeof(double) * (size_t)h->nsh * h->nsh));
+    PG_CUDA(h->d_flist.ensure(std::max<size_t>(h->d_list.bytes, 16)));
+    PG_CUDA(h->d_fcnt.ensure(sizeof(unsigned long long) * 2 * std::max<size_t>(h->work.size(), 1)));
     return 0;
 }
 
@@ -939,25 +1063,24 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
         PG_CUDA(cudaMemcpyAsync(h->d_Pk1.p, P1, sizeof(double) * no2, cudaMemcpyHostToDevice, s));
         unpack_kernel<<<g, 256, 0, s>>>(h->d_Pk1.as<double>(), h->d_D1.as<double>(), h->n);
     }
-    PG_CUDA(cudaMemsetAsync(h->d_A0.p, 0, sizeof(double) * nn, s));
-    if (two) PG_CUDA(cudaMemsetAsync(h->d_A1.p, 0, sizeof(double) * nn, s));
+    if ((rc = acc_clear(h, h->d_A0.p, s))) return rc;
+    if (two && (rc = acc_clear(h, h->d_A1.p, s))) return rc;
     h->last_computed = h->nquart;
-    if (h->tau_dens > 0.0 && h->lists) {
-        rc = density_filter(h, mode == MODE_UHF);
-        if (rc) {
-            h->filtered = false;
-            return rc;
-        }
+    const bool filt = h->tau_dens > 0.0 && h->lists;
+    if (filt) {
+        if ((rc = density_filter_buffers(h))) return rc;
+        if ((rc = density_filter_enqueue(h, mode == MODE_UHF, s))) return rc;
+        h->filtered = true;
+        h->fcnt.assign(2 * std::max<size_t>(h->work.size(), 1), 0);
     }
     rc = launch_fock(h, mode, s);
     h->filtered = false;
     if (rc) return rc;
-    finish_kernel<<<grid_for((long long)no2, h->num_sms), 256, 0, s>>>(h->d_A0.as<double>(), h->d_Gk0.as<double>(),
-                                                                      h->n);
-    if (two)
-        finish_kernel<<<grid_for((long long)no2, h->num_sms), 256, 0, s>>>(h->d_A1.as<double>(),
-                                                                          h->d_Gk1.as<double>(), h->n);
-    PG_CUDA(cudaGetLastError());
+    if (filt)
+        PG_CUDA(cudaMemcpyAsync(h->fcnt.data(), h->d_fcnt.p, sizeof(unsigned long long) * h->fcnt.size(),
+                                cudaMemcpyDeviceToHost, s));
+    if ((rc = finish(h, h->d_A0.as<double>(), h->d_Gk0.as<double>(), s))) return rc;
+    if (two && (rc = finish(h, h->d_A1.as<double>(), h->d_Gk1.as<double>(), s))) return rc;
     h->h_stage.resize(2 * no2);
     PG_CUDA(cudaMemcpyAsync(h->h_stage.data(), h->d_Gk0.p, sizeof(double) * no2, cudaMemcpyDeviceToHost, s));
     if (two)
@@ -966,6 +1089,11 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
     PG_CUDA(cudaStreamSynchronize(s));
     rc = record_timing(h);
     if (rc) return rc;
+    if (filt) {
+        long long tot = 0;
+        for (auto c : h->fcnt) tot += (long long)c;
+        h->last_computed = tot;
+    }
     for (size_t i = 0; i < no2; ++i) G0[i] += h->h_stage[i];
     if (two)
         for (size_t i = 0; i < no2; ++i) G1[i] += h->h_stage[no2 + i];
@@ -1060,6 +1188,16 @@ int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off
                         const double *charge, const double *xyz, int skipcen, double schwarz_tau,
                         patgpu_handle *out)
 {
+    return patgpu_basis_create_quartets(nshell, l, cen, off, nst, prim_off, alpha, coef, ncen, charge, xyz, skipcen,
+                                        schwarz_tau, 0, 0, 1, out);
+}
+
+int patgpu_basis_create_quartets(int nshell, const int *l, const int *cen, const int *off, const int *nst,
+                                 const int *prim_off, const double *alpha, const double *coef, int ncen,
+                                 const double *charge, const double *xyz, int skipcen, double schwarz_tau,
+                                 int start_shell, int rank, int nranks, patgpu_handle *out)
+{
+    if (nranks < 1 || rank < 0 || rank >= nranks) return fail(PATGPU_EINVAL, "bad partition");
     if (!out || nshell < 1 || ncen < 1 || !l || !cen || !off || !nst || !prim_off || !alpha || !coef || !charge ||
         !xyz)
         return fail(PATGPU_EINVAL, "patgpu_basis_create: null or empty argument");
@@ -1094,6 +1232,7 @@ int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off
     h->co.assign(coef, coef + prim_off[nshell]);
     h->q.assign(charge, charge + ncen);
     h->xyz.assign(xyz, xyz + 3 * ncen);
+    if (const char *e = getenv("PATGPU_DETERMINISTIC")) h->det = strcmp(e, "0") ? 1 : 0;
     int dev = 0;
     cudaGetDevice(&dev);
     h->dev = dev;
@@ -1105,6 +1244,9 @@ int patgpu_basis_create(int nshell, const int *l, const int *cen, const int *off
         return fail(PATGPU_ECUDA, "stream/event creation failed");
     }
     cudaMemset(h->d_err.p, 0, sizeof(int));
+    h->start_shell = start_shell;
+    h->rank = rank;
+    h->nranks = nranks;
     rc = build_pairs(h);
     if (!rc) rc = build_schwarz(h);
     if (!rc) rc = build_quartets(h);
@@ -1136,7 +1278,11 @@ int patgpu_set_quartets(patgpu_handle h, int start_shell, int rank, int nranks)
     h->rank = rank;
     h->nranks = nranks;
     int rc = build_quartets(h);
-    return rc ? rc : tune_variants(h);
+    if (!rc) rc = tune_variants(h);
+    // a mixed-precision window set before: count it and tune its kernels
+    // again over the new partition
+    if (!rc && h->tau_mix > 0.0) rc = patgpu_set_mixed_precision(h, h->tau_mix);
+    return rc;
 }
 
 int patgpu_rhf_gmatrix(patgpu_handle h, const double *P, double *G)
@@ -1166,7 +1312,7 @@ int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, 
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nn = (size_t)h->n * h->n;
     unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(dP, h->d_D0.as<double>(), h->n);
-    PG_CUDA(cudaMemsetAsync(dA, 0, sizeof(double) * nn, s));
+    if ((rc = acc_clear(h, dA, s))) return rc;
     EriArgs a = h->base_args();
     a.mode = MODE_RHF;
     a.D0 = h->d_D0.as<double>();
@@ -1185,11 +1331,8 @@ int patgpu_rhf_accumulate_device(patgpu_handle h, const double *dP, double *dA, 
 int patgpu_finish_gmatrix_device(patgpu_handle h, const double *dA, double *dG, void *stream)
 {
     if (!h || !dA || !dG) return fail(PATGPU_EINVAL, "null argument");
-    cudaStream_t s = (cudaStream_t)stream;
-    const long long no2 = (long long)h->n * (h->n + 1) / 2;
-    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(dA, dG, h->n);
-    PG_CUDA(cudaGetLastError());
-    return 0;
+    if (int rc0 = check_device(h)) return rc0;
+    return finish(h, dA, dG, (cudaStream_t)stream);
 }
 
 int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, void *stream)
@@ -1204,17 +1347,18 @@ int patgpu_rhf_gmatrix_device(patgpu_handle h, const double *dP, double *dG, voi
 
 // ------------------------------------------------ allocation-free build
 // patgpu_rhf_gmatrix_device_noalloc keeps its working matrices (the full
-// density and the unsymmetrised accumulator, n*n doubles each) in this
-// fixed array instead of buffers obtained from cudaMalloc.  It is sized for
-// n <= kNoAllocMaxN basis functions: 2 * 512 * 512 doubles = 4 MiB, held by
-// every GPU that loads the library until the process exits.  Host code may
+// density, n*n doubles, and the unsymmetrised accumulator, n*n elements of
+// 16 bytes in the fixed-point mode) in this fixed array instead of buffers
+// obtained from cudaMalloc.  It is sized for n <= kNoAllocMaxN basis
+// functions: 3 * 512 * 512 doubles = 6 MiB, held by every GPU that loads the
+// library until the process exits.  Host code may
 // not use the array's name as a device address; the address is looked up
 // per device with cudaGetSymbolAddress the first time the entry point runs
 // on that device.
 }  // extern "C"
 namespace pg {
 constexpr int kNoAllocMaxN = 512;
-static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxN * kNoAllocMaxN];
+static __device__ __align__(256) double g_noalloc_scratch[3 * kNoAllocMaxN * kNoAllocMaxN];
 constexpr int kNoAllocMaxDevices = 64;
 static std::mutex g_noalloc_lock;
 static double *g_noalloc_ptr[kNoAllocMaxDevices];
@@ -1260,7 +1404,7 @@ int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double 
     // D is fully rewritten; A keeps the previous call's sums and must start at zero
     unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(dP, D, n);
     PG_CUDA(cudaGetLastError());
-    PG_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * nn, s));
+    if ((rc = acc_clear(h, A, s))) return rc;
     EriArgs a = h->base_args();
     a.mode = MODE_RHF;
     a.D0 = D;
@@ -1268,10 +1412,7 @@ int patgpu_rhf_gmatrix_device_noalloc(patgpu_handle h, const double *dP, double 
     for (auto &w : h->work) {
         PG_CUDA(launch_work(h, w, a, s));
     }
-    const long long no2 = (long long)n * (n + 1) / 2;
-    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(A, dG, n);
-    PG_CUDA(cudaGetLastError());
-    return 0;
+    return finish(h, A, dG, s);
 }
 
 int patgpu_eri_quartets(patgpu_handle h, int nq, const int *sh4, double *out)
@@ -1519,6 +1660,20 @@ int patgpu_fp64_peak(double *tflops)
     return 0;
 }
 
+int patgpu_set_deterministic(patgpu_handle h, int on)
+{
+    if (!h) return fail(PATGPU_EINVAL, "null handle");
+    h->det = on ? 1 : 0;
+    return 0;
+}
+
+int patgpu_accumulator_bytes(patgpu_handle h, size_t *bytes)
+{
+    if (!h || !bytes) return fail(PATGPU_EINVAL, "null argument");
+    *bytes = acc_bytes(h);
+    return 0;
+}
+
 int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
 {
     if (!h || !(tau_fp32 >= 0.0)) return fail(PATGPU_EINVAL, "bad mixed-precision threshold");
@@ -1661,6 +1816,15 @@ int patgpu_set_density_screening(patgpu_handle h, double tau_dens)
     return 0;
 }
 
+int patgpu_set_density_precision(patgpu_handle h, double tau32)
+{
+    if (!h || !(tau32 >= 0.0)) return fail(PATGPU_EINVAL, "bad density-weighted precision threshold");
+    if (int rc0 = check_device(h)) return rc0;
+    const bool retune = tau32 > 0.0 && h->tau_dens32 <= 0.0 && h->tau_mix <= 0.0;
+    h->tau_dens32 = tau32;
+    return retune ? tune_fp32(h) : 0;
+}
+
 int patgpu_last_computed(patgpu_handle h, long long *quartets)
 {
     if (!h || !quartets) return fail(PATGPU_EINVAL, "null argument");
@@ -1719,9 +1883,13 @@ struct patgpu_batch_s {
     std::vector<cudaEvent_t> join;
     cudaStream_t cs = nullptr;
     cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int nodes = 0;
+    // [0]: plain builds; [1]: density-screened builds (incremental SCF),
+    // the filter of every molecule inside the graph
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int nodes[2] = {0, 0};
+    int screened = 0;                      // launches use graph [1]
+    double scr_tau = 0.0, scr_tau32 = 0.0; // thresholds graph [1] was captured with
     double last_ns = 0.0;
     std::vector<double> stage;
 };
@@ -1730,40 +1898,52 @@ namespace pg {
 
 constexpr int kBatchStreams = 8;
 
-static void batch_drop_graph(patgpu_batch_s *b)
+static void batch_drop_graph(patgpu_batch_s *b, int which = -1)
 {
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
-    b->nodes = 0;
+    for (int k = 0; k < 2; ++k) {
+        if (which >= 0 && k != which) continue;
+        if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
+        if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
+        b->exec[k] = nullptr;
+        b->graph[k] = nullptr;
+        b->nodes[k] = 0;
+    }
 }
 
-// One molecule's Fock build on stream s from the batch buffers.
-static int batch_enqueue(patgpu_batch_s *b, int m, cudaStream_t s)
+// One molecule's Fock build on stream s from the batch buffers; screened:
+// the density filter of the molecule's handle first, then the class
+// launches over its sublists (counts read on the device).
+static int batch_enqueue(patgpu_batch_s *b, int m, cudaStream_t s, bool screened)
 {
     patgpu_basis *h = b->mols[m];
     const size_t nn = (size_t)h->n * h->n;
-    const long long no2 = (long long)h->n * (h->n + 1) / 2;
     unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(b->dP[m].as<double>(), h->d_D0.as<double>(),
                                                                     h->n);
-    PG_CUDA(cudaMemsetAsync(h->d_A0.p, 0, sizeof(double) * nn, s));
+    if (int rc = acc_clear(h, h->d_A0.p, s)) return rc;
+    const bool filt = screened && h->tau_dens > 0.0 && h->lists;
+    if (filt) {
+        if (int rc = density_filter_enqueue(h, false, s)) return rc;
+        h->filtered = true;
+    }
     EriArgs a = h->base_args();
     a.mode = MODE_RHF;
     a.D0 = h->d_D0.as<double>();
     a.A0 = h->d_A0.as<double>();
-    for (const auto &w : h->work) PG_CUDA(launch_work(h, w, a, s));
-    finish_kernel<<<grid_for(no2, h->num_sms), 256, 0, s>>>(h->d_A0.as<double>(), b->dG[m].as<double>(), h->n);
-    PG_CUDA(cudaGetLastError());
-    return 0;
+    cudaError_t e = cudaSuccess;
+    for (const auto &w : h->work)
+        if (e == cudaSuccess) e = launch_work(h, w, a, s);
+    h->filtered = false;
+    PG_CUDA(e);
+    return finish(h, h->d_A0.as<double>(), b->dG[m].as<double>(), s);
 }
 
-static int batch_capture(patgpu_batch_s *b)
+static int batch_capture(patgpu_batch_s *b, int k)
 {
+    const bool screened = k == 1;
     const int nm = (int)b->mols.size();
     // warm-up outside the capture: configures every kernel it will launch
     for (int m = 0; m < nm; ++m) {
-        int rc = batch_enqueue(b, m, b->cs);
+        int rc = batch_enqueue(b, m, b->cs, screened);
         if (rc) return rc;
     }
     PG_CUDA(cudaStreamSynchronize(b->cs));
@@ -1775,11 +1955,11 @@ static int batch_capture(patgpu_batch_s *b)
     PG_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
     cudaError_t e = cudaEventRecord(b->fork, b->cs);
-    for (size_t k = 0; e == cudaSuccess && k < b->side.size(); ++k) e = cudaStreamWaitEvent(b->side[k], b->fork, 0);
-    for (int k = 0; e == cudaSuccess && !rc && k < nm; ++k) rc = batch_enqueue(b, order[k], b->side[k % b->side.size()]);
-    for (size_t k = 0; e == cudaSuccess && !rc && k < b->side.size(); ++k) {
-        e = cudaEventRecord(b->join[k], b->side[k]);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cs, b->join[k], 0);
+    for (size_t i = 0; e == cudaSuccess && i < b->side.size(); ++i) e = cudaStreamWaitEvent(b->side[i], b->fork, 0);
+    for (int i = 0; e == cudaSuccess && !rc && i < nm; ++i) rc = batch_enqueue(b, order[i], b->side[i % b->side.size()], screened);
+    for (size_t i = 0; e == cudaSuccess && !rc && i < b->side.size(); ++i) {
+        e = cudaEventRecord(b->join[i], b->side[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cs, b->join[i], 0);
     }
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(b->cs, &g);
@@ -1788,11 +1968,11 @@ static int batch_capture(patgpu_batch_s *b)
         if (rc) return rc;
         return fail(PATGPU_ECUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
     }
-    b->graph = g;
-    PG_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+    b->graph[k] = g;
+    PG_CUDA(cudaGraphInstantiate(&b->exec[k], g, 0));
     size_t nodes = 0;
     PG_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
-    b->nodes = (int)nodes;
+    b->nodes[k] = (int)nodes;
     return 0;
 }
 
@@ -1875,16 +2055,53 @@ int patgpu_batch_set_mixed_precision(patgpu_batch b, double tau_fp32)
     return 0;
 }
 
+int patgpu_batch_set_density_screening(patgpu_batch b, double tau_dens, double tau32)
+{
+    if (!b || !(tau_dens >= 0.0) || !(tau32 >= 0.0)) return fail(PATGPU_EINVAL, "bad batch screening threshold");
+    b->screened = tau_dens > 0.0 ? 1 : 0;
+    if (!b->screened) return 0;   // plain graph; the handles' screening stays for graph [1]
+    if (b->exec[1] && tau_dens == b->scr_tau && tau32 == b->scr_tau32) return 0;
+    for (auto *h : b->mols) {
+        int rc = patgpu_set_density_screening(h, tau_dens);
+        if (!rc) rc = patgpu_set_density_precision(h, tau_dens > 0.0 ? tau32 : 0.0);
+        if (!rc && tau_dens > 0.0 && h->lists) rc = density_filter_buffers(h);
+        if (rc) return rc;
+    }
+    b->scr_tau = tau_dens;
+    b->scr_tau32 = tau32;
+    batch_drop_graph(b, 1);
+    return 0;
+}
+
+int patgpu_batch_last_computed(patgpu_batch b, long long *quartets)
+{
+    if (!b || !quartets) return fail(PATGPU_EINVAL, "null argument");
+    long long tot = 0;
+    PG_CUDA(cudaStreamSynchronize(b->cs));
+    for (auto *h : b->mols) {
+        if (!b->screened || !(h->tau_dens > 0.0) || !h->lists) {
+            tot += h->nquart;
+            continue;
+        }
+        std::vector<unsigned long long> c(2 * std::max<size_t>(h->work.size(), 1), 0);
+        PG_CUDA(cudaMemcpy(c.data(), h->d_fcnt.p, sizeof(unsigned long long) * c.size(), cudaMemcpyDeviceToHost));
+        for (auto x : c) tot += (long long)x;
+    }
+    *quartets = tot;
+    return 0;
+}
+
 int patgpu_batch_launch(patgpu_batch b, void *stream)
 {
     if (!b) return fail(PATGPU_EINVAL, "null batch");
-    if (!b->exec) {
-        int rc = batch_capture(b);
+    const int k = b->screened;
+    if (!b->exec[k]) {
+        int rc = batch_capture(b, k);
         if (rc) return rc;
     }
     cudaStream_t s = (cudaStream_t)stream;
     PG_CUDA(cudaEventRecord(b->ev0, s));
-    PG_CUDA(cudaGraphLaunch(b->exec, s));
+    PG_CUDA(cudaGraphLaunch(b->exec[k], s));
     PG_CUDA(cudaEventRecord(b->ev1, s));
     return 0;
 }
@@ -1898,8 +2115,8 @@ int patgpu_batch_rhf_gmatrix(patgpu_batch b, const double *const *P, double *con
         if (!P[m] || !G[m]) return fail(PATGPU_EINVAL, "patgpu_batch_rhf_gmatrix: molecule %d has no matrix", m);
         tot += (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
     }
-    if (!b->exec) {
-        int rc = batch_capture(b);
+    if (!b->exec[b->screened]) {
+        int rc = batch_capture(b, b->screened);
         if (rc) return rc;
     }
     for (int m = 0; m < nm; ++m) {
@@ -1936,7 +2153,7 @@ int patgpu_batch_stats(patgpu_batch b, long long *out4)
     out4[0] = (long long)b->mols.size();
     out4[1] = q;
     out4[2] = q32;
-    out4[3] = b->nodes;
+    out4[3] = b->nodes[b->screened] ? b->nodes[b->screened] : b->nodes[0];
     return 0;
 }
 

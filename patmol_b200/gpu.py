@@ -68,6 +68,8 @@ def lib():
         L.patgpu_rys_host.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.patgpu_fp64_peak.argtypes = [dp]
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
+        L.patgpu_set_deterministic.argtypes = [H, ctypes.c_int]
+        L.patgpu_accumulator_bytes.argtypes = [H, ctypes.POINTER(ctypes.c_size_t)]
         L.patgpu_mixed_stats.argtypes = [H, lp]
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
         L.patgpu_uhf_gradient.argtypes = [H, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp]
@@ -77,6 +79,9 @@ def lib():
         L.patgpu_scf_destroy.argtypes = [H]
         L.patgpu_scf_density_host.argtypes = [H, dp, dp, dp, dp, dp]
         L.patgpu_set_density_screening.argtypes = [H, ctypes.c_double]
+        L.patgpu_set_density_precision.argtypes = [H, ctypes.c_double]
+        L.patgpu_batch_set_density_screening.argtypes = [H, ctypes.c_double, ctypes.c_double]
+        L.patgpu_batch_last_computed.argtypes = [H, lp]
         L.patgpu_last_computed.argtypes = [H, lp]
         L.patgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(H), ctypes.POINTER(H)]
         L.patgpu_batch_destroy.argtypes = [H]
@@ -203,6 +208,18 @@ class GpuBasis:
     def rhf_accumulate_device(self, dP_ptr: int, dA_ptr: int, stream: int):
         _check(lib().patgpu_rhf_accumulate_device(self.h, dP_ptr, dA_ptr, stream), "accumulate")
 
+    def set_deterministic(self, on: bool):
+        """Exact fixed-point J/K accumulation (bitwise reproducible G; the
+        default) or FP64 atomic adds."""
+        _check(lib().patgpu_set_deterministic(self.h, 1 if on else 0), "set_deterministic")
+
+    def accumulator_bytes(self) -> int:
+        """Size of the accumulator rhf_accumulate_device fills (16 n^2 bytes
+        with deterministic accumulation, 8 n^2 without)."""
+        b = ctypes.c_size_t(0)
+        _check(lib().patgpu_accumulator_bytes(self.h, ctypes.byref(b)), "accumulator_bytes")
+        return int(b.value)
+
     def finish_gmatrix_device(self, dA_ptr: int, dG_ptr: int, stream: int):
         _check(lib().patgpu_finish_gmatrix_device(self.h, dA_ptr, dG_ptr, stream), "finish")
 
@@ -255,6 +272,11 @@ class GpuBasis:
         _check(lib().patgpu_last_computed(self.h, ctypes.byref(n)), "patgpu_last_computed")
         return n.value
 
+    def set_density_precision(self, tau32: float):
+        """In density-screened builds, FP32 arithmetic (FP64 sums) for kept
+        quartets whose bound Q_ab Q_cd max|D| is below tau32; 0 turns it off."""
+        _check(lib().patgpu_set_density_precision(self.h, float(tau32)), "set_density_precision")
+
     def set_mixed_precision(self, tau_fp32: float) -> int:
         """FP32 arithmetic for quartets with Schwarz bound below tau_fp32
         (FP64 accumulation); returns how many quartets run in FP32."""
@@ -305,6 +327,17 @@ class GpuBatch:
 
     def set_mixed_precision(self, tau_fp32: float):
         _check(lib().patgpu_batch_set_mixed_precision(self.b, float(tau_fp32)), "batch mixed precision")
+
+    def set_density_screening(self, tau_dens: float, tau32: float = 0.0):
+        """Density screening (and density-weighted FP32, tau32) of every
+        molecule's build: launches then replay the screened graph."""
+        _check(lib().patgpu_batch_set_density_screening(self.b, float(tau_dens), float(tau32)),
+               "batch_set_density_screening")
+
+    def last_computed(self) -> int:
+        n = ctypes.c_longlong()
+        _check(lib().patgpu_batch_last_computed(self.b, ctypes.byref(n)), "batch_last_computed")
+        return n.value
 
     def rhf_form_gmatrix(self, Ps):
         """G_m = G[P_m] for every molecule (packed host arrays)."""

@@ -33,7 +33,10 @@ def run_dropin(tmp_path, basis=None, patin=None, env=None):
 
 
 def test_dropin_water_energy(tmp_path, golden_meta):
-    vals, _ = run_dropin(tmp_path, configs.water_spd())
+    vals, err = run_dropin(tmp_path, configs.water_spd(), env={"PATGPU_VERBOSE": "1"})
+    # the reference's own clean-up at exit (rhfscf.c:15-19) reaches the
+    # library's clean_ERIFS, which frees the handle's device state
+    assert "patgpu: clean_ERIFS released the handle's device state, 0 bound" in err, err[-2000:]
     g = golden_meta["water_spd"]
     # exact-integral energy (reference energy corrected for its root2 defect)
     assert abs(vals[1] - g["e_total_exact_integrals"]) < 5e-9

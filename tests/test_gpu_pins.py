@@ -19,8 +19,10 @@ number at the size of that term.
     term at its converged density.
   * He + DPM through the drop-in program: the reference's dpmvpol.dat value
     and ground-state energy, 1e-9 Eh.
-  * Converged SCF energies of small molecules of the batched family against
-    the reference's SCF: FP64 within 1e-8 Eh, mixed precision within 1e-6 Eh.
+  * Converged SCF energies of small molecules of the batched family: FP64
+    within 1e-9 Eh and mixed precision within 1e-6 Eh of the oracle's
+    converged energy; the reference's own energy plus its first-order defect
+    term within 5e-5 Eh.
   * Analytic nuclear gradients of the converged SCF against central
     differences (h = 1e-4 bohr) of the reference's own SCF energies, with and
     without DPM: 1e-6 Eh/bohr.
@@ -70,7 +72,7 @@ def test_c1_full_gmatrix_and_energy(which, c1_handle, pins):
     fx = golden("water_spdf_g.npz")
     meta = pins["c1"]
     if which == "seeded":
-        P = seeded_density(n, meta["seeded"]["seed"], meta["seeded"]["scale"])
+        P = seeded_density(n, meta["seeded_density"]["seed"], meta["seeded_density"]["scale"])
     else:
         P = fx["P_core_guess"]
     G = g.rhf_form_gmatrix(P)
@@ -126,17 +128,26 @@ def test_he_dpm_dropin_vpol(tmp_path, golden_meta):
 # ----------------------------------------- converged SCF energies, FP64 and mixed
 @pytest.mark.parametrize("natom,seed", MOLS)
 def test_scf_energy_vs_reference(natom, seed, pins):
+    """FP64 within 1e-9 Eh and mixed precision within 1e-6 Eh of the oracle's
+    converged energy (exact quadrature).  The reference's own converged energy
+    differs from it by the reference's root defect, up to 2.2e-4 Eh on these
+    molecules; the first-order term tr(P dG) at the reference's density
+    accounts for most of it and leaves up to 3.5e-5 Eh (second order: the
+    defect also moves the converged density)."""
     rec = next(r for r in pins["mols"] if r["natom"] == natom and r["seed"] == seed)
+    assert rec["oracle_scf"]["converged"]
     b = configs.organic_basis(natom, seed, with_f=False)
     g = gpu.GpuBasis(b)
-    e64 = scf.rhf(b, gpu=g)
-    emx = scf.rhf(b, gpu=g, tau_fp32=1e-8)
+    e64 = scf.rhf(b, gpu=g, conv=1e-11, maxit=200)
+    emx = scf.rhf(b, gpu=g, tau_fp32=1e-8, conv=1e-11, maxit=200)
     g.close()
     assert e64.converged and emx.converged
-    exact = rec["e_total_exact_integrals"]
-    assert abs(e64.energy - exact) < 1e-8, (e64.energy, exact, rec)
+    exact = rec["oracle_scf"]["e_total"]
+    assert abs(e64.energy - exact) < 1e-9, (e64.energy, exact, rec)
     assert abs(emx.energy - exact) < 1e-6, (emx.energy, exact)
-    assert abs(emx.energy - rec["scf"]["e_total"]) < 1e-6
+    ref = rec["scf"]["e_total"] + rec["de_root_defect_first_order"]
+    assert abs(e64.energy - ref) < 5e-5, (e64.energy, ref)
+    assert abs(e64.energy - rec["scf"]["e_total"]) < 5e-4
 
 
 # --------------------------------------------- gradients vs the reference's FD

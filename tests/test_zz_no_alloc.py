@@ -49,6 +49,22 @@ def test_noalloc_matches_allocating_build_two_calls():
     assert np.abs(n1 - n2).max() > 1e-3          # the densities differ, so must G
 
 
+def test_noalloc_matches_allocating_build_mixed_precision():
+    """With the mixed-precision window on, the class launches take their
+    two-window and one-launch forms; the allocation-free build must follow
+    them exactly like the allocating one."""
+    b = configs.water_spd()
+    G = gpu.GpuBasis(b)
+    assert G.set_mixed_precision(1e-8) >= 0
+    P = seeded_density(b.norb, 33)
+    n1 = _device_build(G, G.rhf_gmatrix_device_noalloc, P)
+    r1 = _device_build(G, G.rhf_gmatrix_device, P)
+    n2 = _device_build(G, G.rhf_gmatrix_device_noalloc, P)
+    assert np.all(np.isfinite(n1))
+    assert np.abs(n1 - r1).max() < 1e-11
+    assert n1.tobytes() == n2.tobytes()
+
+
 def test_noalloc_rejects_bases_beyond_its_scratch():
     # 52 f shells = 520 functions, above the 512 the fixed scratch holds
     specs = [(3, k % 2, [0.3 * 1.5 ** (k // 2)], [1.0]) for k in range(52)]
