@@ -62,6 +62,11 @@ def parse():
     ap.add_argument("--batch-max-atoms", type=int, default=8,
                     help="molecule sizes of the batched leg are uniform in 3..this")
     ap.add_argument("--alkane-carbons", type=int, default=12)
+    ap.add_argument("--scf-molecules", type=int, default=12,
+                    help="molecules of the SCF-iteration leg (config-3 recipe); 0 skips it")
+    ap.add_argument("--scf-max-atoms", type=int, default=24,
+                    help="molecule sizes of the SCF-iteration leg are uniform in 3..this")
+    ap.add_argument("--no-organic40", action="store_true", help="skip the 40-atom (config-2) leg")
     ap.add_argument("--scf-iters", type=int, default=3,
                     help="alkane_dpm: SCF iterations before the gradient (timing; the converged "
                          "finite-difference check runs at C3H8 size in the GPU tests)")
@@ -251,6 +256,53 @@ def scf_leg(torch):
         g.close()
     out["dE_incremental_vs_full"] = out["incremental"]["energy"] - out["full"]["energy"]
     return out
+
+
+def scf_iteration_leg(a, torch):
+    """Batched-SCF throughput (the metric's s/SCF-iteration on the config-3
+    recipe): a seeded sample of molecules of 3..max atoms (C/N/O/H walk,
+    config-0 s/p/d basis) converged two ways:
+      plain: one molecule after the other, every iteration a full FP64 Fock
+             build (patgpu_rhf_gmatrix), host DIIS and diagonalisation;
+      mixed: all molecules in lock step, one CUDA-graph launch per iteration
+             (patgpu_batch), Schwarz-bound FP32 window below tau_fp32 in full
+             builds, density-screened difference builds in between with
+             density-weighted FP32 while the density still moves (the final
+             iterations' difference builds stay FP64), full build every 8.
+    SCF iterations per second of each (molecule-iterations / wall seconds,
+    host steps included) and every molecule's |E_mixed - E_plain|."""
+    import numpy as np
+    from patmol_b200 import configs, scf
+    rng = np.random.default_rng(303)
+    sizes = rng.integers(3, a.scf_max_atoms + 1, size=a.scf_molecules)
+    bases = [configs.organic_basis(int(k), 3000 + i, with_f=False) for i, k in enumerate(sizes)]
+    kw = dict(conv=1e-10, comm_tol=1e-6, dp_tol=1e-6, maxit=60)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    plain = [scf.rhf(b, **kw) for b in bases]
+    t_plain = time.time() - t0
+    it_plain = sum(r.iterations for r in plain)
+    computed = []
+    t0 = time.time()
+    mixed = scf.rhf_batch(bases, tau_fp32=a.tau_fp32, incremental=True, tau_inc=1e-11, tau_inc32=1e-5,
+                          computed=computed, **kw)
+    t_mixed = time.time() - t0
+    it_mixed = sum(r.iterations for r in mixed)
+    dE = [abs(x.energy - y.energy) for x, y in zip(plain, mixed)]
+    thr_plain, thr_mixed = it_plain / t_plain, it_mixed / t_mixed
+    return {"workload": f"{a.scf_molecules} seeded molecules of 3-{a.scf_max_atoms} atoms (C/N/O/H walk), config-0 "
+                        "s/p/d basis, RHF converged to dE < 1e-10 Eh, max|FPS-SPF| < 1e-6",
+            "atoms": [int(x) for x in sizes], "basis_functions": [b.norb for b in bases],
+            "plain_fp64": {"seconds": t_plain, "iterations": it_plain, "scf_iterations_per_s": thr_plain,
+                           "s_per_scf_iteration": t_plain / it_plain,
+                           "converged": sum(r.converged for r in plain)},
+            "mixed_batched": {"seconds": t_mixed, "iterations": it_mixed, "scf_iterations_per_s": thr_mixed,
+                              "s_per_scf_iteration": t_mixed / it_mixed,
+                              "converged": sum(r.converged for r in mixed), "tau_fp32": a.tau_fp32,
+                              "tau_inc": 1e-11, "tau_inc32": 1e-5, "lockstep_iterations": len(computed),
+                              "quartets_per_build": computed},
+            "scf_iteration_speedup": thr_mixed / thr_plain,
+            "max_abs_dE": max(dE), "dE_per_molecule": dE}
 
 
 def linalg_leg():
@@ -582,6 +634,14 @@ def main():
         if world == 1:
             line["scf"] = scf_leg(torch)
             line["linalg"] = linalg_leg()
+            if not a.no_organic40:
+                o = organic40_leg(a, torch, stream)
+                line["organic40"] = {"workload": o["config"]["workload"], "basis_functions": o["config"]["basis_functions"],
+                                     "quartets": o["config"]["quartets"], "ms_per_fock_build_fp64": o["ms_per_step"],
+                                     "quartets_per_s_fp64": o["value"], "roofline": o["roofline"], "mixed": o["mixed"],
+                                     "setup_s": o["config"]["setup_s"]}
+            if a.scf_molecules > 0:
+                line["scf_iteration"] = scf_iteration_leg(a, torch)
         if world == 1 and not a.no_cpu_baseline:
             res, err = reference_fock(2, 1)
             line["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}

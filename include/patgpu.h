@@ -74,6 +74,12 @@ void one_electron_ints(double *Smat, double *Tmat, double *Hmat);
  * keeps e allocated. */
 void clean_ERIFS(ERIFS *e);
 
+/* Replaces momints (momints.h:11, momints.c:88-188): writes MOMINTS.DAT in
+ * the working directory with the reference's records -- per shell pair
+ * (ish >= jsh) and component pair (j <= i), int i, int j, the three dipole
+ * and six quadrupole integrals -- computed on the GPU. */
+void momints(void);
+
 /* ------------------------------------------------------------- explicit */
 typedef struct patgpu_basis *patgpu_handle;
 
@@ -185,6 +191,13 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
                    const int *prim_off, const double *alpha, const double *coef, int ncen,
                    const double *charge, const double *xyz, int skipcen, double *S, double *T,
                    double *H, double *Hdpm);
+
+/* Moment integrals about the coordinate origin, replacing the integrals of
+ * momints (momints.h:11, momints.c:13-188): dip[3][no2] (x, y, z) and
+ * quad[6][no2] (xx, xy, xz, yy, yz, zz), packed lower triangles with the
+ * reference's component order and factors, overwritten.  No handle. */
+int patgpu_moments(int nshell, const int *l, const int *cen, const int *off, const int *nst, const int *prim_off,
+                   const double *alpha, const double *coef, int ncen, const double *xyz, double *dip, double *quad);
 
 /* Nuclear gradient of the closed-shell SCF energy (no counterpart in the
  * reference, which has no gradients):

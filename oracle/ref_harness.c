@@ -5,6 +5,7 @@
  * dumps into the current directory, which must hold patin.dat (and
  * posgrid.dat for "scf" with dpm on).  Nothing in the product links this.
  *
+ *   ref_harness moments         MOMINTS.DAT (the reference's momints, momints.c:88-188)
  *   ref_harness ints            S.bin T.bin H.bin (packed lower triangle),
  *                               eri.bin (ERINT records, erifs.h:19-22),
  *                               info.txt (norb nshell ncen enuc nrec)
@@ -27,6 +28,7 @@
  *                               first ERI file (a bounded sample of the
  *                               Fock build), after W untimed calls.
  */
+#include "momints.h"
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -460,6 +462,11 @@ int main(int argc, char **argv)
                 enuc_nonzero(), nrec, secs);
         fclose(f);
         clean_ERIFS(e);
+        return 0;
+    }
+    if (!strcmp(argv[1], "moments")) {
+        /* the reference's moment integrals (momints.c:88-188), MOMINTS.DAT */
+        momints();
         return 0;
     }
     if (!strcmp(argv[1], "gmat") && argc >= 3) {

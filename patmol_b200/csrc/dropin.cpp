@@ -6,6 +6,7 @@
 // the library also loads in programs that have no reference basis module
 // (the explicit patgpu_* layer needs none), in which case these entry
 // points report the missing accessors through fatalError.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -194,6 +195,40 @@ void uhf_form_gmatrix(const ERIFS *tfiles, const double *PmatA, const double *Pm
     auto it = g_handles.find(tfiles);
     if (it == g_handles.end()) die("uhf_form_gmatrix before two_electron_ints");
     if (it->second && patgpu_uhf_gmatrix(it->second, PmatA, PmatB, GmatA, GmatB)) die("uhf_form_gmatrix");
+}
+
+void momints(void)
+{
+    select_device_once();
+    Snap s = snapshot();
+    int n = 0;
+    for (int i = 0; i < s.nsh; ++i)
+        if (s.nst[i]) n = std::max(n, s.off[i] + s.nst[i]);
+    const size_t no2 = (size_t)n * (n + 1) / 2;
+    std::vector<double> dip(3 * no2), quad(6 * no2);
+    if (patgpu_moments(s.nsh, s.l.data(), s.cen.data(), s.off.data(), s.nst.data(), s.poff.data(), s.al.data(),
+                       s.co.data(), s.ncen, s.xyz.data(), dip.data(), quad.data()))
+        die("momints");
+    // the reference's record stream (momints.c:131-179)
+    FILE *f = fopen("MOMINTS.DAT", "wb");
+    if (!f) die("momints: cannot create MOMINTS.DAT");
+    for (int ish = 0; ish < s.nsh; ++ish)
+        for (int jsh = 0; jsh <= ish; ++jsh)
+            for (int a = 0; a < s.nst[ish]; ++a) {
+                const int ir = s.off[ish] + a;
+                for (int b = 0; b < s.nst[jsh]; ++b) {
+                    const int jr = s.off[jsh] + b;
+                    if (jr > ir) break;
+                    const size_t ij = (size_t)ir * (ir + 1) / 2 + jr;
+                    double v[9];
+                    for (int k = 0; k < 3; ++k) v[k] = dip[k * no2 + ij];
+                    for (int k = 0; k < 6; ++k) v[3 + k] = quad[k * no2 + ij];
+                    if (fwrite(&ir, sizeof(int), 1, f) != 1 || fwrite(&jr, sizeof(int), 1, f) != 1 ||
+                        fwrite(v, sizeof(double), 9, f) != 9)
+                        die("momints: writing MOMINTS.DAT");
+                }
+            }
+    if (fclose(f)) die("momints: closing MOMINTS.DAT");
 }
 
 void dpm_ints(double *hmat)

@@ -141,25 +141,31 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                 const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
                 for (int f = lt; f < 2 * NR; f += NL) s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg);
             }
-            // stage the density blocks, component factors folded in
+            // stage D(ab) (every lane reads all of it), and with the exchange
+            // densities kept in shared memory also D(bd), D(bc), D(ad), D(ac);
+            // component factors folded in
 #pragma unroll
             for (int s = 0; s < NDEN; ++s) {
                 const double *D = s == 0 ? args.D0 : args.D1;
                 double *db = s_db + s * NDB;
-                for (int t = lt; t < NDB; t += NL) {
-                    int r0, c0, lr, lc2, ir, icn;
-                    if (t < S::OBD) {
-                        ir = t / NB; icn = t - ir * NB; r0 = fa; c0 = fb; lr = LA; lc2 = LB;
-                    } else if (t < S::OBC) {
-                        const int tt = t - S::OBD; ir = tt / ND; icn = tt - ir * ND; r0 = fb; c0 = fd; lr = LB; lc2 = LD;
-                    } else if (t < S::OAD) {
-                        const int tt = t - S::OBC; ir = tt / NC; icn = tt - ir * NC; r0 = fb; c0 = fc; lr = LB; lc2 = LC;
-                    } else if (t < S::OAC) {
-                        const int tt = t - S::OAD; ir = tt / ND; icn = tt - ir * ND; r0 = fa; c0 = fd; lr = LA; lc2 = LD;
-                    } else {
-                        const int tt = t - S::OAC; ir = tt / NC; icn = tt - ir * NC; r0 = fa; c0 = fc; lr = LA; lc2 = LC;
+                for (int t = lt; t < NAB; t += NL) {
+                    const int ir = t / NB, icn = t - (t / NB) * NB;
+                    db[t] = __ldg(D + (size_t)(fa + ir) * n + fb + icn) * c_norm[LA][ir] * c_norm[LB][icn];
+                }
+                if constexpr (!S::DREG) {
+                    for (int t = lt + S::OBD; t < NDB; t += NL) {
+                        int r0, c0, lr, lc2, ir, icn;
+                        if (t < S::OBC) {
+                            const int tt = t - S::OBD; ir = tt / ND; icn = tt - ir * ND; r0 = fb; c0 = fd; lr = LB; lc2 = LD;
+                        } else if (t < S::OAD) {
+                            const int tt = t - S::OBC; ir = tt / NC; icn = tt - ir * NC; r0 = fb; c0 = fc; lr = LB; lc2 = LC;
+                        } else if (t < S::OAC) {
+                            const int tt = t - S::OAD; ir = tt / ND; icn = tt - ir * ND; r0 = fa; c0 = fd; lr = LA; lc2 = LD;
+                        } else {
+                            const int tt = t - S::OAC; ir = tt / NC; icn = tt - ir * NC; r0 = fa; c0 = fc; lr = LA; lc2 = LC;
+                        }
+                        db[t] = __ldg(D + (size_t)(r0 + ir) * n + c0 + icn) * c_norm[lr][ir] * c_norm[lc2][icn];
                     }
-                    db[t] = __ldg(D + (size_t)(r0 + ir) * n + c0 + icn) * c_norm[lr][ir] * c_norm[lc2][icn];
                 }
             }
         }
@@ -215,18 +221,21 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
             if (NDEN == 2) Dcd += __ldg(args.D1 + (size_t)(fc + ic) * n + fd + id);
             Dcd *= nfk;
             if constexpr (S::DREG) {
+                // this lane's exchange densities straight from the n x n
+                // density (consecutive ket components read consecutive words)
+                const double nd = c_norm[LD][id], nc = c_norm[LC][ic];
 #pragma unroll
                 for (int s = 0; s < NDEN; ++s) {
-                    const double *db = s_db + s * NDB;
+                    const double *D = s == 0 ? args.D0 : args.D1;
 #pragma unroll
                     for (int b = 0; b < NB; ++b) {
-                        dbd[s][b] = db[S::OBD + b * ND + id];
-                        dbc[s][b] = db[S::OBC + b * NC + ic];
+                        dbd[s][b] = __ldg(D + (size_t)(fb + b) * n + fd + id) * (c_norm[LB][b] * nd);
+                        dbc[s][b] = __ldg(D + (size_t)(fb + b) * n + fc + ic) * (c_norm[LB][b] * nc);
                     }
 #pragma unroll
                     for (int a = 0; a < NA; ++a) {
-                        dad[s][a] = db[S::OAD + a * ND + id];
-                        dac[s][a] = db[S::OAC + a * NC + ic];
+                        dad[s][a] = __ldg(D + (size_t)(fa + a) * n + fd + id) * (c_norm[LA][a] * nd);
+                        dac[s][a] = __ldg(D + (size_t)(fa + a) * n + fc + ic) * (c_norm[LA][a] * nc);
                     }
                 }
             }
@@ -335,34 +344,45 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
             }
             __syncwarp();
             if (work) {
-                constexpr int T1 = NA * NC, T2 = T1 + NA * ND, T3 = T2 + NB * NC, T4 = T3 + NB * ND;
-                for (int t = lt; t < T4; t += NL) {
-                    int row, col, base2, stride2, cnt, off, lr, lc2, ir, icl;
-                    if (t < T1) {          // K(a,c) = sum_d Pac[(c,d)][a]
-                        ir = t / NC; icl = t - ir * NC;
-                        row = fa + ir; col = fc + icl; base2 = icl * ND; stride2 = 1; cnt = ND; off = ir;
-                        lr = LA; lc2 = LC;
-                    } else if (t < T2) {   // K(a,d) = sum_c Pad[(c,d)][a]
-                        const int tt = t - T1; ir = tt / ND; icl = tt - ir * ND;
-                        row = fa + ir; col = fd + icl; base2 = icl; stride2 = ND; cnt = NC; off = NA + ir;
-                        lr = LA; lc2 = LD;
-                    } else if (t < T3) {   // K(b,c) = sum_d Pbc[(c,d)][b]
-                        const int tt = t - T2; ir = tt / NC; icl = tt - ir * NC;
-                        row = fb + ir; col = fc + icl; base2 = icl * ND; stride2 = 1; cnt = ND; off = 2 * NA + ir;
-                        lr = LB; lc2 = LC;
-                    } else {               // K(b,d) = sum_c Pbd[(c,d)][b]
-                        const int tt = t - T3; ir = tt / ND; icl = tt - ir * ND;
-                        row = fb + ir; col = fd + icl; base2 = icl; stride2 = ND; cnt = NC; off = 2 * NA + NB + ir;
-                        lr = LB; lc2 = LD;
-                    }
-                    const double f = sK * c_norm[lr][ir] * c_norm[lc2][icl];
-                    const size_t idx = (size_t)row * n + col;
+                // K(a,c) = sum_d Pac, K(a,d) = sum_c Pad, K(b,c) = sum_d Pbc,
+                // K(b,d) = sum_c Pbd over the team's ket components (lane
+                // c*ND + d holds the partials of ket component (c, d))
 #pragma unroll
-                    for (int s = 0; s < NDEN; ++s) {
+                for (int s = 0; s < NDEN; ++s) {
+                    double *A = mode == MODE_JK ? args.A1 : (s == 0 ? args.A0 : args.A1);
+                    const double sg = mode == MODE_JK ? sK : -sK;
+                    const double *pp = s_part + (size_t)s * NL * PS;
+                    for (int t = lt; t < NA * NC; t += NL) {
+                        const int a = t / NC, c = t - (t / NC) * NC;
                         double sum = 0.0;
-                        for (int k = 0; k < cnt; ++k) sum += s_part[((size_t)s * NL + base2 + k * stride2) * PS + off];
-                        if (mode == MODE_JK) acc_add(args.A1, idx, f * sum, args.det, args.err);
-                        else acc_add(s == 0 ? args.A0 : args.A1, idx, -f * sum, args.det, args.err);
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) sum += pp[(c * ND + d) * PS + a];
+                        acc_add(A, (size_t)(fa + a) * n + fc + c, sg * c_norm[LA][a] * c_norm[LC][c] * sum, args.det,
+                                args.err);
+                    }
+                    for (int t = lt; t < NA * ND; t += NL) {
+                        const int a = t / ND, d = t - (t / ND) * ND;
+                        double sum = 0.0;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) sum += pp[(c * ND + d) * PS + NA + a];
+                        acc_add(A, (size_t)(fa + a) * n + fd + d, sg * c_norm[LA][a] * c_norm[LD][d] * sum, args.det,
+                                args.err);
+                    }
+                    for (int t = lt; t < NB * NC; t += NL) {
+                        const int b = t / NC, c = t - (t / NC) * NC;
+                        double sum = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) sum += pp[(c * ND + d) * PS + 2 * NA + b];
+                        acc_add(A, (size_t)(fb + b) * n + fc + c, sg * c_norm[LB][b] * c_norm[LC][c] * sum, args.det,
+                                args.err);
+                    }
+                    for (int t = lt; t < NB * ND; t += NL) {
+                        const int b = t / ND, d = t - (t / ND) * ND;
+                        double sum = 0.0;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) sum += pp[(c * ND + d) * PS + 2 * NA + NB + b];
+                        acc_add(A, (size_t)(fb + b) * n + fd + d, sg * c_norm[LB][b] * c_norm[LD][d] * sum, args.det,
+                                args.err);
                     }
                 }
             }

@@ -1779,6 +1779,25 @@ int patgpu_onebody(int nshell, const int *l, const int *cen, const int *off, con
                        nullptr);
 }
 
+int patgpu_moments(int nshell, const int *l, const int *cen, const int *off, const int *nst, const int *prim_off,
+                   const double *alpha, const double *coef, int ncen, const double *xyz, double *dip, double *quad)
+{
+    if (nshell < 1 || !l || !cen || !off || !nst || !prim_off || !alpha || !coef || !xyz || !dip || !quad)
+        return fail(PATGPU_EINVAL, "patgpu_moments: null argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(PATGPU_ENODEV, "no CUDA device: the GPU library has no CPU path");
+    int n = 0;
+    for (int s = 0; s < nshell; ++s) {
+        if (nst[s] && (l[s] < 0 || l[s] > PG_LMAX))
+            return fail(PATGPU_EUNSUPPORTED, "shell %d has l = %d; the kernels support l <= %d", s, l[s], PG_LMAX);
+        if (nst[s]) n = std::max(n, off[s] + nst[s]);
+    }
+    int rc = init_tables();
+    if (rc) return rc;
+    return run_moments(nshell, l, cen, off, nst, prim_off, alpha, coef, ncen, xyz, n, dip, quad, nullptr);
+}
+
 int patgpu_uhf_gradient(patgpu_handle h, const double *PA, const double *PB, const double *WA, const double *WB,
                         int parts, int with_dpm, double *grad)
 {

@@ -199,6 +199,129 @@ __global__ void onebody_kernel(const OneArgs a)
     if (a.V) a.V[ij] = dv;
 }
 
+// ------------------------------------------------------------- moments
+// Dipole and quadrupole integrals about the coordinate origin (the
+// quantities momints.c:13-85 forms), one thread per component pair.  With
+// the Hermite expansion of the pair about P, the one-dimensional moments are
+//   M0 = E_0,  M1 = E_1 + P E_0,  M2 = 2 E_2 + 2 P E_1 + (P^2 + 1/(2p)) E_0
+// (times sqrt(pi/p)), and a three-dimensional moment is the product of the
+// per-direction factors: x = M1x M0y M0z, xy = M1x M1y M0z, xx = M2x M0y M0z.
+struct MomArgs {
+    const int *item;     // per thread: ish, jsh, ia, ib, packed index
+    int nitem;
+    const int *l, *cen, *poff;
+    const double *al, *co, *xyz;
+    size_t no2;
+    double *out;         // [9][no2]: x, y, z, then xx, xy, xz, yy, yz, zz
+};
+
+__global__ void moments_kernel(const MomArgs a)
+{
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= a.nitem) return;
+    const int ish = a.item[5 * it], jsh = a.item[5 * it + 1], ia = a.item[5 * it + 2], ib = a.item[5 * it + 3];
+    const int ij = a.item[5 * it + 4];
+    const int la = a.l[ish], lb = a.l[jsh];
+    const int ca = c_cart1[la][ia], cb = c_cart1[lb][ib];
+    const int ex[3] = {ca & 15, (ca >> 4) & 15, ca >> 8};
+    const int eb[3] = {cb & 15, (cb >> 4) & 15, cb >> 8};
+    const double *A = a.xyz + 3 * a.cen[ish], *B = a.xyz + 3 * a.cen[jsh];
+    const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+    const double ab2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    const double nrm = c_norm1[la][ia] * c_norm1[lb][ib];
+    const double PI32 = 5.568327996831707845;      // pi^(3/2)
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double E[3][EM][EM][ET];
+    for (int i = a.poff[ish]; i < a.poff[ish + 1]; ++i)
+        for (int j = a.poff[jsh]; j < a.poff[jsh + 1]; ++j) {
+            const double ea = a.al[i], ebx = a.al[j], p = ea + ebx;
+            const double w = a.co[i] * a.co[j] * nrm * PI32 * exp(-ea * ebx * ab2 / p) / (p * sqrt(p));
+            double m0[3], m1[3], m2[3];
+            for (int d = 0; d < 3; ++d) {
+                const double P = (ea * A[d] + ebx * B[d]) / p;
+                // E up to t = ex + eb + 2, zero above ex + eb
+                herm_e(E[d], ex[d] + 1, eb[d] + 1, 0.5 / p, P - A[d], P - B[d]);
+                const double *e = E[d][ex[d]][eb[d]];
+                m0[d] = e[0];
+                m1[d] = e[1] + P * e[0];
+                m2[d] = 2.0 * e[2] + 2.0 * P * e[1] + (P * P + 0.5 / p) * e[0];
+            }
+            acc[0] += w * m1[0] * m0[1] * m0[2];
+            acc[1] += w * m0[0] * m1[1] * m0[2];
+            acc[2] += w * m0[0] * m0[1] * m1[2];
+            acc[3] += w * m2[0] * m0[1] * m0[2];
+            acc[4] += w * m1[0] * m1[1] * m0[2];
+            acc[5] += w * m1[0] * m0[1] * m1[2];
+            acc[6] += w * m0[0] * m2[1] * m0[2];
+            acc[7] += w * m0[0] * m1[1] * m1[2];
+            acc[8] += w * m0[0] * m0[1] * m2[2];
+        }
+    for (int k = 0; k < 9; ++k) a.out[k * a.no2 + ij] = acc[k];
+}
+
+int run_moments(int nsh, const int *l, const int *cen, const int *off, const int *nst, const int *poff,
+                const double *al, const double *co, int ncen, const double *xyz, int n, double *dip, double *quad,
+                cudaStream_t s)
+{
+    std::vector<int> items;
+    for (int i = 0; i < nsh; ++i) {
+        if (!nst[i]) continue;
+        for (int j = 0; j <= i; ++j) {
+            if (!nst[j]) continue;
+            for (int ia = 0; ia < nst[i]; ++ia)
+                for (int ib = 0; ib < nst[j]; ++ib) {
+                    const int ir = off[i] + ia, jr = off[j] + ib;
+                    if (jr > ir) continue;
+                    items.insert(items.end(), {i, j, ia, ib, ir * (ir + 1) / 2 + jr});
+                }
+        }
+    }
+    const int nitem = (int)items.size() / 5;
+    const size_t no2 = (size_t)n * (n + 1) / 2;
+    const int np = poff[nsh];
+    void *d_item = nullptr, *d_l = nullptr, *d_cen = nullptr, *d_poff = nullptr, *d_al = nullptr, *d_co = nullptr,
+         *d_xyz = nullptr, *d_out = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](void **d, const void *h, size_t b) {
+        if (e != cudaSuccess) return;
+        e = cudaMalloc(d, b ? b : 16);
+        if (e == cudaSuccess && b) e = cudaMemcpyAsync(*d, h, b, cudaMemcpyHostToDevice, s);
+    };
+    up(&d_item, items.data(), sizeof(int) * items.size());
+    up(&d_l, l, sizeof(int) * nsh);
+    up(&d_cen, cen, sizeof(int) * nsh);
+    up(&d_poff, poff, sizeof(int) * (nsh + 1));
+    up(&d_al, al, sizeof(double) * np);
+    up(&d_co, co, sizeof(double) * np);
+    up(&d_xyz, xyz, sizeof(double) * 3 * ncen);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(double) * no2 * 9);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_out, 0, sizeof(double) * no2 * 9, s);
+    if (e == cudaSuccess && nitem) {
+        MomArgs a{};
+        a.item = (const int *)d_item;
+        a.nitem = nitem;
+        a.l = (const int *)d_l;
+        a.cen = (const int *)d_cen;
+        a.poff = (const int *)d_poff;
+        a.al = (const double *)d_al;
+        a.co = (const double *)d_co;
+        a.xyz = (const double *)d_xyz;
+        a.no2 = no2;
+        a.out = (double *)d_out;
+        moments_kernel<<<(nitem + 127) / 128, 128, 0, s>>>(a);
+        e = cudaGetLastError();
+    }
+    std::vector<double> h(no2 * 9);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_out, sizeof(double) * no2 * 9, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    for (void *p : {d_item, d_l, d_cen, d_poff, d_al, d_co, d_xyz, d_out})
+        if (p) cudaFree(p);
+    if (e != cudaSuccess) return fail(PATGPU_ECUDA, "moment integrals: %s", cudaGetErrorString(e));
+    for (size_t k = 0; k < 3 * no2; ++k) dip[k] = h[k];
+    for (size_t k = 0; k < 6 * no2; ++k) quad[k] = h[3 * no2 + k];
+    return 0;
+}
+
 int run_oneints(int nsh, const int *l, const int *cen, const int *off, const int *nst, const int *poff,
                 const double *al, const double *co, int ncen, const double *q, const double *xyz, int skipcen,
                 int n, double *S, double *T, double *H, double *Hdpm, cudaStream_t s)

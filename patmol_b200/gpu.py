@@ -69,6 +69,7 @@ def lib():
         L.patgpu_fp64_peak.argtypes = [dp]
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_set_deterministic.argtypes = [H, ctypes.c_int]
+        L.patgpu_moments.argtypes = [ctypes.c_int, ip, ip, ip, ip, ip, dp, dp, ctypes.c_int, dp, dp, dp]
         L.patgpu_accumulator_bytes.argtypes = [H, ctypes.POINTER(ctypes.c_size_t)]
         L.patgpu_mixed_stats.argtypes = [H, lp]
         L.patgpu_rhf_gradient.argtypes = [H, dp, dp, ctypes.c_int, ctypes.c_int, dp]
@@ -412,6 +413,20 @@ def read_eri_files(prefix: str, basename: str, rank: int, nfiles: int):
     """Concatenated records of ERI files f = 0 .. nfiles-1 (ERINT layout, erifs.h:19-22)."""
     parts = [np.fromfile(f"{prefix}{rank}{f}{basename}", dtype=ERINT_DTYPE) for f in range(nfiles)]
     return np.concatenate(parts) if parts else np.zeros(0, dtype=ERINT_DTYPE)
+
+
+def moments(basis):
+    """Dipole (3, no2) and quadrupole (6, no2: xx, xy, xz, yy, yz, zz)
+    integrals about the origin, packed (patgpu_moments, momints.c)."""
+    f = basis.flat_arrays()
+    no2 = basis.norb * (basis.norb + 1) // 2
+    dip = np.zeros(3 * no2)
+    quad = np.zeros(6 * no2)
+    _check(lib().patgpu_moments(basis.nshell, _p(f["l"], ctypes.c_int), _p(f["cen"], ctypes.c_int),
+                                _p(f["off"], ctypes.c_int), _p(f["nst"], ctypes.c_int),
+                                _p(f["prim_off"], ctypes.c_int), _p(f["alpha"]), _p(f["coef"]), basis.ncen,
+                                _p(f["coords"]), _p(dip), _p(quad)), "patgpu_moments")
+    return dip.reshape(3, no2), quad.reshape(6, no2)
 
 
 def onebody(basis, want_sth=True, Hdpm=None):

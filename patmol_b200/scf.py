@@ -59,7 +59,8 @@ def orthogonalizer(S: np.ndarray, smin: float = 1e-10) -> np.ndarray:
 class _RHFState:
     """One molecule's closed-shell iteration (host side of rhf_scf_update)."""
 
-    def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float, device_linalg: bool = False):
+    def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float, device_linalg: bool = False,
+                 comm_tol: float = 1e-9, dp_tol: float = 1e-8):
         if basis.nelec % 2 or basis.mult != 1:
             raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
         self.n = basis.norb
@@ -68,6 +69,7 @@ class _RHFState:
         self.X = orthogonalizer(self.S)
         self.enuc = nuclear_repulsion(basis)
         self.ndiis, self.conv = ndiis, conv
+        self.comm_tol, self.dp_tol = comm_tol, dp_tol
         # the step of rhf_scf_update after F (X^T F X, diagonalise, C, P) on the
         # GPU (patgpu_scf_*) or on the host
         self.linalg = GpuScfLinalg(self.X, self.nocc) if device_linalg else None
@@ -119,8 +121,9 @@ class _RHFState:
         self.eps, C, P_new = self.diag_density(F)
         dP = float(np.max(np.abs(P_new - self.P)))
         self.P = P_new
+        self.dP = dP
         if self.e_old is not None and abs(energy - self.e_old) < self.conv and \
-                float(np.max(np.abs(self.es[-1]))) < 1e-9 and dP < 1e-8:
+                float(np.max(np.abs(self.es[-1]))) < self.comm_tol and dP < self.dp_tol:
             self.converged = True
         self.e_old = energy
 
@@ -154,10 +157,16 @@ class IncrementalFock:
     difference build (patgpu_set_density_screening at tau_inc; the default
     1e-14 drops contributions at the level below which the reference stores
     no integral, twoints.c:375), and a full unscreened build every
-    `full_every` iterations.  Records the quartets each build computed."""
+    `full_every` iterations.  tau32 > 0: while the density still changes by
+    more than fp32_dp_min (early iterations), quartets of a difference build
+    whose density-weighted bound is below tau32 run in FP32; the difference
+    builds of the final iterations stay FP64.  Records the quartets each
+    build computed."""
 
-    def __init__(self, gb: GpuBasis, tau_inc: float = 1e-14, full_every: int = 8):
+    def __init__(self, gb: GpuBasis, tau_inc: float = 1e-14, full_every: int = 8, tau32: float = 0.0,
+                 fp32_dp_min: float = 1e-4):
         self.gb, self.tau_inc, self.full_every = gb, tau_inc, full_every
+        self.tau32, self.fp32_dp_min = tau32, fp32_dp_min
         self.P = self.G = None
         self.n = 0
         self.computed = []
@@ -168,9 +177,12 @@ class IncrementalFock:
             gb.set_density_screening(0.0)
             G = gb.rhf_form_gmatrix(Pp)
         else:
+            dP = Pp - self.P
             gb.set_density_screening(self.tau_inc)
-            G = self.G + gb.rhf_form_gmatrix(Pp - self.P)
+            gb.set_density_precision(self.tau32 if float(np.abs(dP).max()) > self.fp32_dp_min else 0.0)
+            G = self.G + gb.rhf_form_gmatrix(dP)
             gb.set_density_screening(0.0)
+            gb.set_density_precision(0.0)
         self.computed.append(gb.last_computed())
         self.n += 1
         self.P, self.G = Pp.copy(), G
@@ -179,7 +191,8 @@ class IncrementalFock:
 
 def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
         maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
-        tau_inc: float = 1e-14, device_linalg: bool = False, tau_fp32: float = 0.0) -> RHFResult:
+        tau_inc: float = 1e-14, device_linalg: bool = False, tau_fp32: float = 0.0, tau_inc32: float = 0.0,
+        comm_tol: float = 1e-9, dp_tol: float = 1e-8) -> RHFResult:
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
     from a full build.  device_linalg=True diagonalises on the GPU.
@@ -189,8 +202,8 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
     Sp, Hp = _setup(gb, dpm)
     if tau_fp32 > 0.0:
         gb.set_mixed_precision(tau_fp32)
-    st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg)
-    fock = IncrementalFock(gb, tau_inc) if incremental else None
+    st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg, comm_tol=comm_tol, dp_tol=dp_tol)
+    fock = IncrementalFock(gb, tau_inc, tau32=tau_inc32) if incremental else None
     while st.it < maxit and not st.converged:
         Pp = st.packed_density()
         st.step(fock(Pp) if fock else gb.rhf_form_gmatrix(Pp))
@@ -204,26 +217,49 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
 
 
 def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-12, maxit: int = 100,
-              schwarz_tau: float = 1e-14, ndiis: int = 8):
+              schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False, tau_inc: float = 1e-11,
+              tau_inc32: float = 0.0, fp32_dp_min: float = 1e-4, full_every: int = 8, comm_tol: float = 1e-9,
+              dp_tol: float = 1e-8, computed: list | None = None):
     """Closed-shell SCF of many molecules in lock step: every iteration is one
     batched Fock build (one CUDA graph over all molecules, patgpu_batch_*),
     then each molecule's host step.  Converged molecules keep their density.
-    tau_fp32 > 0 runs quartets with Schwarz bound below it in FP32."""
+    tau_fp32 > 0 runs quartets with Schwarz bound below it in FP32.
+    incremental=True: between full builds (the first and every full_every-th
+    iteration) the graph builds G[P_n - P_(n-1)] of every molecule with
+    density screening at tau_inc (the filter runs inside the graph) and adds
+    it to the previous G; while a molecule's density still changes by more
+    than fp32_dp_min, tau_inc32 > 0 also runs its kept quartets with a
+    density-weighted bound below tau_inc32 in FP32 (the difference builds of
+    the final iterations stay FP64).  The final energies come from a full
+    build.  computed, if given, receives the quartets of every build."""
     gbs = [GpuBasis(b, schwarz_tau=schwarz_tau) for b in bases]
     states = []
     for b, gb in zip(bases, gbs):
         Sp, Hp = _setup(gb, dpm)
-        states.append(_RHFState(b, Sp, Hp, ndiis, conv))
+        states.append(_RHFState(b, Sp, Hp, ndiis, conv, comm_tol=comm_tol, dp_tol=dp_tol))
     batch = GpuBatch(gbs)
     if tau_fp32 > 0.0:
         batch.set_mixed_precision(tau_fp32)
     it = 0
+    Gprev = Pprev = None
     while it < maxit and not all(st.converged for st in states):
         it += 1
-        Gs = batch.rhf_form_gmatrix([st.packed_density() for st in states])
+        Ps = [st.packed_density() for st in states]
+        if not incremental or Gprev is None or (it - 1) % full_every == 0:
+            batch.set_density_screening(0.0)
+            Gs = batch.rhf_form_gmatrix(Ps)
+        else:
+            dPs = [P - Pp for P, Pp in zip(Ps, Pprev)]
+            big = max(float(np.abs(d).max()) for d in dPs)
+            batch.set_density_screening(tau_inc, tau_inc32 if big > fp32_dp_min else 0.0)
+            Gs = [Gp + dG for Gp, dG in zip(Gprev, batch.rhf_form_gmatrix(dPs))]
+        if computed is not None:
+            computed.append(batch.last_computed())
+        Gprev, Pprev = Gs, Ps
         for st, G in zip(states, Gs):
             if not st.converged:
                 st.step(G)
+    batch.set_density_screening(0.0)
     Gs = batch.rhf_form_gmatrix([st.packed_density() for st in states])
     out = [st.finish(G) for st, G in zip(states, Gs)]
     batch.close()

@@ -28,6 +28,8 @@ Parts (each writes its own files and merges its entry into pins.json):
   gradfd   Central differences (h = 1e-4 bohr) of the reference's own SCF
            energies for the gradient pins: closed-shell water and water with
            the DPM potential (positron displaced too).
+  moments  The reference's MOMINTS.DAT records (momints.c:88-188) for the
+           contracted s/p/d/f mini basis and water s/p/d.
   org      The oracle's converged SCF energy of an 8-atom molecule of the
            40-atom family (s/p/d/f on every atom): DIIS SCF on the CPU
            restatement's G builds (slow: hours on 8 cores).
@@ -272,6 +274,28 @@ def part_gradfd():
     merge("gradfd", recs)
 
 
+MOM_DTYPE = np.dtype([("i", "<i4"), ("j", "<i4"), ("dip", "<f8", 3), ("quad", "<f8", 6)])
+
+
+def ref_moments(basis):
+    """The reference's MOMINTS.DAT records (momints.c:88-188) for a basis."""
+    with tempfile.TemporaryDirectory(prefix="patref_mom_") as d:
+        basis.write_patin(os.path.join(d, "patin.dat"))
+        subprocess.run([os.path.join(ROOT, "oracle", "_ref", "ref_harness"), "moments"], cwd=d, check=True,
+                       capture_output=True)
+        return np.fromfile(os.path.join(d, "MOMINTS.DAT"), dtype=MOM_DTYPE)
+
+
+def part_moments():
+    from golden.make_golden import mini_basis
+    arrays = {}
+    for name, b in (("mini", mini_basis()), ("water_spd", configs.water_spd())):
+        r = ref_moments(b)
+        arrays.update({f"{name}_i": r["i"], f"{name}_j": r["j"], f"{name}_dip": r["dip"], f"{name}_quad": r["quad"]})
+        print(name, len(r), flush=True)
+    np.savez_compressed(os.path.join(OUT, "moments.npz"), **arrays)
+
+
 def part_org():
     from patmol_b200.scf import _RHFState
     natom, seed = int(os.environ.get("PINS_ORG_NATOM", "8")), int(os.environ.get("PINS_ORG_SEED", "3"))
@@ -295,7 +319,8 @@ def part_org():
 def main(argv):
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "restatement",
                     f"REF={reference_tree()}"], check=True)
-    parts = {"c1": part_c1, "sf6": part_sf6, "mols": part_mols, "gradfd": part_gradfd, "org": part_org}
+    parts = {"c1": part_c1, "sf6": part_sf6, "mols": part_mols, "gradfd": part_gradfd, "org": part_org,
+             "moments": part_moments}
     for p in argv or list(parts):
         parts[p]()
 
