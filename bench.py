@@ -263,45 +263,53 @@ def scf_iteration_leg(a, torch):
     recipe): a seeded sample of molecules of 3..max atoms (C/N/O/H walk,
     config-0 s/p/d basis) converged two ways:
       plain: one molecule after the other, every iteration a full FP64 Fock
-             build (patgpu_rhf_gmatrix), host DIIS and diagonalisation;
+             build (patgpu_rhf_gmatrix);
       mixed: all molecules in lock step, one CUDA-graph launch per iteration
              (patgpu_batch), Schwarz-bound FP32 window below tau_fp32 in full
              builds, density-screened difference builds in between with
              density-weighted FP32 while the density still moves (the final
              iterations' difference builds stay FP64), full build every 8.
-    SCF iterations per second of each (molecule-iterations / wall seconds,
-    host steps included) and every molecule's |E_mixed - E_plain|."""
+    Both use DIIS, the device eigensolver and canonical orthogonalisation
+    over overlap eigenvalues above 1e-7 (the diffuse 0.08 s exponents on
+    atoms 2.6-2.9 bohr apart make the overlap nearly singular; the same
+    space for both).  Reported: SCF iterations per second of the Fock builds
+    (device-timed; the metric) and of the whole SCF (wall, host steps
+    included), and every molecule's |E_mixed - E_plain|."""
     import numpy as np
     from patmol_b200 import configs, scf
     rng = np.random.default_rng(303)
     sizes = rng.integers(3, a.scf_max_atoms + 1, size=a.scf_molecules)
     bases = [configs.organic_basis(int(k), 3000 + i, with_f=False) for i, k in enumerate(sizes)]
-    kw = dict(conv=1e-10, comm_tol=1e-6, dp_tol=1e-6, maxit=60)
+    kw = dict(conv=1e-10, comm_tol=1e-6, dp_tol=1e-6, maxit=80, smin=1e-7, device_linalg=True)
     torch.cuda.synchronize()
     t0 = time.time()
     plain = [scf.rhf(b, **kw) for b in bases]
     t_plain = time.time() - t0
     it_plain = sum(r.iterations for r in plain)
-    computed = []
+    fock_plain = sum(r.fock_seconds for r in plain)
+    computed, fock_b = [], []
     t0 = time.time()
-    mixed = scf.rhf_batch(bases, tau_fp32=a.tau_fp32, incremental=True, tau_inc=1e-11, tau_inc32=1e-5,
-                          computed=computed, **kw)
+    mixed = scf.rhf_batch(bases, tau_fp32=a.tau_fp32, incremental=True, tau_inc=1e-10, tau_inc32=1e-6,
+                          computed=computed, fock_seconds=fock_b, **kw)
     t_mixed = time.time() - t0
     it_mixed = sum(r.iterations for r in mixed)
+    fock_mixed = sum(fock_b)
     dE = [abs(x.energy - y.energy) for x, y in zip(plain, mixed)]
-    thr_plain, thr_mixed = it_plain / t_plain, it_mixed / t_mixed
     return {"workload": f"{a.scf_molecules} seeded molecules of 3-{a.scf_max_atoms} atoms (C/N/O/H walk), config-0 "
                         "s/p/d basis, RHF converged to dE < 1e-10 Eh, max|FPS-SPF| < 1e-6",
             "atoms": [int(x) for x in sizes], "basis_functions": [b.norb for b in bases],
-            "plain_fp64": {"seconds": t_plain, "iterations": it_plain, "scf_iterations_per_s": thr_plain,
-                           "s_per_scf_iteration": t_plain / it_plain,
-                           "converged": sum(r.converged for r in plain)},
-            "mixed_batched": {"seconds": t_mixed, "iterations": it_mixed, "scf_iterations_per_s": thr_mixed,
-                              "s_per_scf_iteration": t_mixed / it_mixed,
-                              "converged": sum(r.converged for r in mixed), "tau_fp32": a.tau_fp32,
-                              "tau_inc": 1e-11, "tau_inc32": 1e-5, "lockstep_iterations": len(computed),
+            "plain_fp64": {"wall_s": t_plain, "fock_s": fock_plain, "iterations": it_plain,
+                           "fock_s_per_scf_iteration": fock_plain / it_plain,
+                           "wall_s_per_scf_iteration": t_plain / it_plain,
+                           "converged": int(sum(r.converged for r in plain))},
+            "mixed_batched": {"wall_s": t_mixed, "fock_s": fock_mixed, "iterations": it_mixed,
+                              "fock_s_per_scf_iteration": fock_mixed / it_mixed,
+                              "wall_s_per_scf_iteration": t_mixed / it_mixed,
+                              "converged": int(sum(r.converged for r in mixed)), "tau_fp32": a.tau_fp32,
+                              "tau_inc": 1e-10, "tau_inc32": 1e-6, "lockstep_iterations": len(computed),
                               "quartets_per_build": computed},
-            "scf_iteration_speedup": thr_mixed / thr_plain,
+            "scf_iteration_speedup_fock": (it_mixed / fock_mixed) / (it_plain / fock_plain),
+            "scf_iteration_speedup_wall": (it_mixed / t_mixed) / (it_plain / t_plain),
             "max_abs_dE": max(dE), "dE_per_molecule": dE}
 
 
@@ -597,6 +605,7 @@ def main():
     line = None
     if rank == 0:
         peak = gpu.fp64_peak_tflops()
+        dmma = gpu.dmma_peak_tflops()
         achieved = my_flops / (kern_ms * 1e-3) / 1e12 if kern_ms > 0 else None
         line = {
             "metric": "ERI quartets/s (Fock build)",
@@ -621,6 +630,9 @@ def main():
                          "frac": (achieved / peak) if achieved else None, "traffic": STEP_DRAM_BYTES,
                          "traffic_source": STEP_DRAM_SOURCE,
                          "peak_source": "measured FP64 FMA probe (patgpu_fp64_peak), this GPU, this run",
+                         "fp64_mma_tflops": dmma,
+                         "fp64_mma_source": "measured mma.sync m8n8k4 FP64 probe (patgpu_dmma_peak), this GPU, "
+                                            "this run: the only FP64 tensor-core path on sm_100a",
                          "algorithmic_flops_per_step": my_flops,
                          "kernel_ms_per_step": kern_ms},
             "mixed": {"tau_fp32": a.tau_fp32, "fp32_quartets": int(nfp32_t.item()),

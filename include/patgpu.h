@@ -347,6 +347,10 @@ int patgpu_last_timing(patgpu_handle h, double *kernel_ns, int *launches);
 /* Measured dense FP64 FMA throughput of the current device (TFLOP/s), the
  * denominator of the kernels' roofline fraction. */
 int patgpu_fp64_peak(double *tflops);
+/* Dense FP64 matrix-instruction rate of the current GPU in TFLOP/s
+ * (mma.sync m8n8k4, 8 independent accumulators per thread), to set beside
+ * patgpu_fp64_peak: on sm_100a this is the only FP64 tensor-core form. */
+int patgpu_dmma_peak(double *tflops);
 
 /* Host evaluation of the Rys root tables the kernels use (no device
  * needed): x = t^2 nodes and weights of the n-point rule at T. */

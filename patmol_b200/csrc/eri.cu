@@ -101,7 +101,7 @@ cudaError_t launch_eri_class(int LA, int LB, int LC, int LD, const EriArgs &a, c
         // the warp kernels take one density set, Fock modes only and one
         // primitive pair per shell pair; elsewhere the lane kernel (FP64) or
         // the shared-memory kernel (FP32) serves
-        if (a.mode != MODE_UHF && a.mode != MODE_EXPORT && a.single_prim) {
+        if (a.mode != MODE_UHF && a.mode != MODE_EXPORT && a.single_prim && a.ppk) {
 #define PG_WARP(la, lb, lc, ld, sw)                                                             \
     if ((sw == 0 && LA == la && LB == lb && LC == lc && LD == ld) ||                           \
         (sw == 1 && LA == lc && LB == ld && LC == la && LD == lb)) {                           \

@@ -40,8 +40,9 @@ struct EriArgs {
     // least start_shell.
     int implicit;
     int u0, nu, v0, nv, same, rank, nranks, start_shell;
-    // compacted mode (implicit and klist set): item qi is class quartet
-    // klist[qi], already screened; no window test
+    // compacted mode (implicit and klist set): item qi is the quartet
+    // klist[qi] = bra pair | ket pair << 32 (global pair indices), already
+    // screened and partitioned; no window test
     const unsigned long long *klist;
     const double *Q;
     double tau_lo, tau_hi;
@@ -57,6 +58,11 @@ struct EriArgs {
     double prim_cut;        // skip primitive quartets whose coefficient-free
                             // prefactor is below this (1e-15 = twoints.c:110)
     int *err;               // device error word (0 = ok)
+    // one-primitive handles: per pair 16 doubles in one 128-byte line -- p,
+    // P (3), K, the coefficient-free prefactor, A (3), A - B (3), then the
+    // first functions fa | fb << 32 and the shells sa | sb << 32 as 64-bit
+    // integers (read by the warp kernel)
+    const double *ppk;
     int det;                // 1: A0/A1 are fixed-point accumulators (acc_add)
     // device work count: with nq_dev set, the launch runs *nq_dev items (a
     // count an earlier kernel on the stream wrote; nquart is then only the
@@ -149,8 +155,12 @@ __device__ __forceinline__ bool eri_quartet_at(const EriArgs &a, long long qi, i
         const int2 q = a.quart[qi];
         ub = q.x;
         vk = q.y;
+    } else if (a.klist) {
+        const unsigned long long e = __ldg(a.klist + qi);
+        ub = (int)(unsigned)(e & 0xffffffffull);
+        vk = (int)(unsigned)(e >> 32);
     } else {
-        const long long k = a.klist ? (long long)__ldg(a.klist + qi) : qi * a.nranks + a.rank;
+        const long long k = qi * a.nranks + a.rank;
         long long i, j;
         if (a.same) {
             i = (long long)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
@@ -165,13 +175,11 @@ __device__ __forceinline__ bool eri_quartet_at(const EriArgs &a, long long qi, i
         }
         ub = a.u0 + (int)i;
         vk = a.v0 + (int)j;
-        if (!a.klist) {
-            const double b = __ldg(a.Q + ub) * __ldg(a.Q + vk);
-            if (!(b >= a.tau_lo && b < a.tau_hi)) return false;
-            if (a.start_shell > 0 &&
-                max(max(a.pr.sa[ub], a.pr.sb[ub]), max(a.pr.sa[vk], a.pr.sb[vk])) < a.start_shell)
-                return false;
-        }
+        const double b = __ldg(a.Q + ub) * __ldg(a.Q + vk);
+        if (!(b >= a.tau_lo && b < a.tau_hi)) return false;
+        if (a.start_shell > 0 &&
+            max(max(a.pr.sa[ub], a.pr.sb[ub]), max(a.pr.sa[vk], a.pr.sb[vk])) < a.start_shell)
+            return false;
     }
     u = a.swap ? vk : ub;
     v = a.swap ? ub : vk;

@@ -17,7 +17,8 @@
 //     D(b,c), D(a,d) and D(a,c) over the bra components, are read into
 //     registers once per quartet (for bras of up to 9 components), so the
 //     digestion's FMAs take no shared-memory operand.
-//   * 1/p, 1/q and 1/(p+q) are formed once per quartet.
+//   * 1/p, 1/q and 1/(p+q) are formed once per quartet, and each pair's
+//     data is one 128-byte record (EriArgs::ppk) read with 128-bit loads.
 //
 // Per quartet and team: (A) pair data, the staged density blocks (component
 // factors folded in) and the 2n Chebyshev series of the roots and weights;
@@ -120,23 +121,36 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
         double ppq = 1.0, p = 1.0, q = 1.0, sr = 0.0;
         double pax = 0, pay = 0, paz = 0, qcx = 0, qcy = 0, qcz = 0, pqx = 0, pqy = 0, pqz = 0;
         double abx = 0, aby = 0, abz = 0, cdx = 0, cdy = 0, cdz = 0;
+        bool sab = false, scd = false;
         if (active) {
-            fa = __ldg(args.pr.fa + u); fb = __ldg(args.pr.fb + u);
-            fc = __ldg(args.pr.fa + v); fd = __ldg(args.pr.fb + v);
-            const int ib = __ldg(args.pr.pstart + u), ik = __ldg(args.pr.pstart + v);
-            abx = __ldg(args.pr.abx + u); aby = __ldg(args.pr.aby + u); abz = __ldg(args.pr.abz + u);
-            cdx = __ldg(args.pr.abx + v); cdy = __ldg(args.pr.aby + v); cdz = __ldg(args.pr.abz + v);
-            p = __ldg(args.pp.p + ib);
-            q = __ldg(args.pp.p + ik);
-            const double Px = __ldg(args.pp.px + ib), Py = __ldg(args.pp.py + ib), Pz = __ldg(args.pp.pz + ib);
-            const double Qx = __ldg(args.pp.px + ik), Qy = __ldg(args.pp.py + ik), Qz = __ldg(args.pp.pz + ik);
+            // the packed pair records: one 128-byte line per pair (EriArgs::ppk)
+            const double2 *Rb = reinterpret_cast<const double2 *>(args.ppk) + 8 * (size_t)u;
+            const double2 *Rk = reinterpret_cast<const double2 *>(args.ppk) + 8 * (size_t)v;
+            const double2 b0 = __ldg(Rb), b1 = __ldg(Rb + 1), b2 = __ldg(Rb + 2), b3 = __ldg(Rb + 3);
+            const double2 b4 = __ldg(Rb + 4), b5 = __ldg(Rb + 5), b6 = __ldg(Rb + 6);
+            const double2 k0 = __ldg(Rk), k1 = __ldg(Rk + 1), k2 = __ldg(Rk + 2), k3 = __ldg(Rk + 3);
+            const double2 k4 = __ldg(Rk + 4), k5 = __ldg(Rk + 5), k6 = __ldg(Rk + 6);
+            const unsigned long long fab = (unsigned long long)__double_as_longlong(b6.x);
+            const unsigned long long fcd = (unsigned long long)__double_as_longlong(k6.x);
+            const unsigned long long sb2 = (unsigned long long)__double_as_longlong(b6.y);
+            const unsigned long long sk2 = (unsigned long long)__double_as_longlong(k6.y);
+            fa = (int)(unsigned)(fab & 0xffffffffull); fb = (int)(unsigned)(fab >> 32);
+            fc = (int)(unsigned)(fcd & 0xffffffffull); fd = (int)(unsigned)(fcd >> 32);
+            sab = (sb2 & 0xffffffffull) == (sb2 >> 32);
+            scd = (sk2 & 0xffffffffull) == (sk2 >> 32);
+            abx = b4.y; aby = b5.x; abz = b5.y;
+            cdx = k4.y; cdy = k5.x; cdz = k5.y;
+            p = b0.x;
+            q = k0.x;
+            const double Px = b0.y, Py = b1.x, Pz = b1.y;
+            const double Qx = k0.y, Qy = k1.x, Qz = k1.y;
             ppq = p + q;
             const double rs = rsqrt(ppq);
             // the primitive cut of twoints.c:109-111 drops the whole quartet
-            if (kSR * __ldg(args.pp.cut + ib) * __ldg(args.pp.cut + ik) * rs >= args.prim_cut) {
-                sr = kSR * __ldg(args.pp.K + ib) * __ldg(args.pp.K + ik) * rs;
-                pax = Px - __ldg(args.pr.ax + u); pay = Py - __ldg(args.pr.ay + u); paz = Pz - __ldg(args.pr.az + u);
-                qcx = Qx - __ldg(args.pr.ax + v); qcy = Qy - __ldg(args.pr.ay + v); qcz = Qz - __ldg(args.pr.az + v);
+            if (kSR * b2.y * k2.y * rs >= args.prim_cut) {
+                sr = kSR * b2.x * k2.x * rs;
+                pax = Px - b3.x; pay = Py - b3.y; paz = Pz - b4.x;
+                qcx = Qx - k3.x; qcy = Qy - k3.y; qcz = Qz - k4.x;
                 pqx = Px - Qx; pqy = Py - Qy; pqz = Pz - Qz;
                 const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
                 for (int f = lt; f < 2 * NR; f += NL) s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg);
@@ -200,8 +214,8 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
         __syncwarp();
 
         // ------------------------------------------------------ digestion
-        const bool sab = work && __ldg(args.pr.sa + u) == __ldg(args.pr.sb + u);
-        const bool scd = work && __ldg(args.pr.sa + v) == __ldg(args.pr.sb + v);
+        sab = sab && work;
+        scd = scd && work;
         const double deg = (sab ? 1.0 : 2.0) * (scd ? 1.0 : 2.0) * (u == v ? 1.0 : 2.0);
         const double sJ = mode == MODE_RHF ? 0.5 * deg : 0.25 * deg;
         const double sK = 0.125 * deg;

@@ -161,6 +161,7 @@ struct patgpu_basis {
     pg::DBuf d_psa, d_psb, d_pfa, d_pfb, d_pax, d_pay, d_paz, d_pabx, d_paby, d_pabz, d_pstart, d_pnum;
     pg::DBuf d_pp_p, d_pp_px, d_pp_py, d_pp_pz, d_pp_K, d_pp_cut, d_Q;
     pg::DBuf d_pca, d_pcb, d_pp_ea;
+    pg::DBuf d_ppk;                  // packed pair records (one-primitive handles)
     // quartets
     std::vector<pg::ClassWork> work;
     long long nquart = 0, nquart_unscreened = 0;
@@ -211,6 +212,7 @@ struct patgpu_basis {
         a.single_prim = single_prim ? 1 : 0;
         a.err = d_err.as<int>();
         a.det = det;
+        a.ppk = single_prim ? d_ppk.as<double>() : nullptr;
         return a;
     }
 };
@@ -283,6 +285,25 @@ static int build_pairs(patgpu_basis *h)
     UP(d_pp_p, pp_p); UP(d_pp_px, pp_px); UP(d_pp_py, pp_py); UP(d_pp_pz, pp_pz); UP(d_pp_K, pp_K);
     UP(d_pp_cut, pp_cut);
     UP(d_pca, pca); UP(d_pcb, pcb); UP(d_pp_ea, pp_ea);
+    if (h->single_prim) {
+        // one 128-byte record per pair (EriArgs::ppk)
+        std::vector<double> pk(16 * (size_t)h->npair, 0.0);
+        for (int u = 0; u < h->npair; ++u) {
+            double *r = &pk[16 * (size_t)u];
+            const int ip = h->pstart[u];
+            r[0] = h->pp_p[ip]; r[1] = h->pp_px[ip]; r[2] = h->pp_py[ip]; r[3] = h->pp_pz[ip];
+            r[4] = h->pp_K[ip]; r[5] = h->pp_cut[ip];
+            r[6] = h->pax[u]; r[7] = h->pay[u]; r[8] = h->paz[u];
+            r[9] = h->pabx[u]; r[10] = h->paby[u]; r[11] = h->pabz[u];
+            const unsigned long long f = (unsigned long long)(unsigned)h->pfa[u] |
+                                         ((unsigned long long)(unsigned)h->pfb[u] << 32);
+            const unsigned long long sh = (unsigned long long)(unsigned)h->psa[u] |
+                                          ((unsigned long long)(unsigned)h->psb[u] << 32);
+            memcpy(&r[12], &f, 8);
+            memcpy(&r[13], &sh, 8);
+        }
+        if (e == cudaSuccess) e = upload(h->d_ppk, pk, s);
+    }
 #undef UP
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(PATGPU_ECUDA, "pair upload: %s", cudaGetErrorString(e));
@@ -473,7 +494,8 @@ __global__ void count_kernel(const EriArgs a, unsigned long long *cnt)
 }
 
 // Stream compaction of one window of a class's implicit quartet space: the
-// class index k of every surviving item, appended at out[*cursor++] with
+// (bra pair, ket pair) of every surviving item, packed as u | v << 32 and
+// appended at out[*cursor++] with
 // warp-aggregated atomics (order within a warp kept).
 __global__ void compact_kernel(const EriArgs a, unsigned long long *out, unsigned long long *cursor)
 {
@@ -488,11 +510,14 @@ __global__ void compact_kernel(const EriArgs a, unsigned long long *out, unsigne
         unsigned long long base = 0;
         if (lane == lead) base = atomicAdd(cursor, (unsigned long long)__popc(m));
         base = __shfl_sync(0xffffffffu, base, lead);
-        if (keep) out[base + __popc(m & ((1u << lane) - 1u))] = (unsigned long long)(qi * a.nranks + a.rank);
+        if (keep)
+            out[base + __popc(m & ((1u << lane) - 1u))] =
+                (unsigned long long)(unsigned)u | ((unsigned long long)(unsigned)v << 32);
     }
 }
 
-// Compacted quartet lists (8 bytes per surviving quartet), when they fit in
+// Compacted quartet lists (8 bytes per surviving quartet: bra pair | ket
+// pair << 32), when they fit in
 // half of the free device memory above a reserve of a tenth of the device
 // and PATGPU_LISTS is not 0: the class
 // kernels then visit only surviving quartets instead of stepping their
@@ -848,6 +873,28 @@ __global__ void fma_probe_kernel(double *out, int iters, double a, double b)
     if (s == 1234.5678) out[0] = s;   // keeps the chains alive
 }
 
+// FP64 matrix instructions (mma.sync m8n8k4, the only FP64 tensor-core form
+// sm_100a has; tcgen05.mma has no FP64 kind): 8 independent accumulator
+// pairs per thread, `iters` steps each, 512 flops per warp instruction.
+__global__ void dmma_probe_kernel(double *out, int iters, double a, double b)
+{
+    double c[8][2];
+    for (int k = 0; k < 8; ++k) {
+        c[k][0] = threadIdx.x * 1e-9 + k;
+        c[k][1] = c[k][0] + 0.5;
+    }
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                         : "+d"(c[k][0]), "+d"(c[k][1])
+                         : "d"(a), "d"(b));
+    }
+    double s = 0.0;
+    for (int k = 0; k < 8; ++k) s += c[k][0] + c[k][1];
+    if (s == 1234.5678) out[0] = s;   // keeps the chains alive
+}
+
 static int grid_for(long long work, int num_sms)
 {
     long long b = (work + 255) / 256;
@@ -855,7 +902,9 @@ static int grid_for(long long work, int num_sms)
     return (int)std::max<long long>(1, std::min(b, cap));
 }
 
-static int launch_fock(patgpu_basis *h, int mode, cudaStream_t s)
+// The class launches of one build; timing starts here unless the caller
+// recorded ev0 already (a density-screened build times its filter too).
+static int launch_fock(patgpu_basis *h, int mode, cudaStream_t s, bool timed_before = false)
 {
     EriArgs a = h->base_args();
     a.mode = mode;
@@ -863,7 +912,7 @@ static int launch_fock(patgpu_basis *h, int mode, cudaStream_t s)
     a.D1 = h->d_D1.as<double>();
     a.A0 = h->d_A0.as<double>();
     a.A1 = h->d_A1.as<double>();
-    PG_CUDA(cudaEventRecord(h->ev0, s));
+    if (!timed_before) PG_CUDA(cudaEventRecord(h->ev0, s));
     int launches = 0;
     for (auto &w : h->work) {
         PG_CUDA(launch_work(h, w, a, s));
@@ -1069,11 +1118,12 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
     const bool filt = h->tau_dens > 0.0 && h->lists;
     if (filt) {
         if ((rc = density_filter_buffers(h))) return rc;
+        PG_CUDA(cudaEventRecord(h->ev0, s));
         if ((rc = density_filter_enqueue(h, mode == MODE_UHF, s))) return rc;
         h->filtered = true;
         h->fcnt.assign(2 * std::max<size_t>(h->work.size(), 1), 0);
     }
-    rc = launch_fock(h, mode, s);
+    rc = launch_fock(h, mode, s, filt);
     h->filtered = false;
     if (rc) return rc;
     if (filt)
@@ -1657,6 +1707,34 @@ int patgpu_fp64_peak(double *tflops)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *tflops = 4.0 * 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+    return 0;
+}
+
+int patgpu_dmma_peak(double *tflops)
+{
+    if (!tflops) return fail(PATGPU_EINVAL, "null argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(PATGPU_ENODEV, "no CUDA device");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    DBuf out;
+    PG_CUDA(out.ensure(sizeof(double)));
+    cudaEvent_t e0, e1;
+    PG_CUDA(cudaEventCreate(&e0));
+    PG_CUDA(cudaEventCreate(&e1));
+    const int iters = 1 << 12, threads = 256, blocks = sms * 8;
+    dmma_probe_kernel<<<blocks, threads>>>(out.as<double>(), iters, 0.999999999, 1e-9);   // warm-up
+    PG_CUDA(cudaEventRecord(e0));
+    for (int r = 0; r < 4; ++r) dmma_probe_kernel<<<blocks, threads>>>(out.as<double>(), iters, 0.999999999, 1e-9);
+    PG_CUDA(cudaEventRecord(e1));
+    PG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double warps = (double)threads / 32.0 * blocks;
+    *tflops = 4.0 * 512.0 * 8.0 * iters * warps / (ms * 1e-3) / 1e12;
     return 0;
 }
 

@@ -67,6 +67,7 @@ def lib():
         L.patgpu_last_timing.argtypes = [H, dp, ip]
         L.patgpu_rys_host.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.patgpu_fp64_peak.argtypes = [dp]
+        L.patgpu_dmma_peak.argtypes = [dp]
         L.patgpu_set_mixed_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_set_deterministic.argtypes = [H, ctypes.c_int]
         L.patgpu_moments.argtypes = [ctypes.c_int, ip, ip, ip, ip, ip, dp, dp, ctypes.c_int, dp, dp, dp]
@@ -110,6 +111,13 @@ def fp64_peak_tflops() -> float:
     v = ctypes.c_double()
     _check(lib().patgpu_fp64_peak(ctypes.byref(v)), "patgpu_fp64_peak")
     return v.value
+
+
+def dmma_peak_tflops() -> float:
+    """FP64 mma.sync (DMMA) rate of this GPU, TFLOP/s."""
+    t = ctypes.c_double()
+    _check(lib().patgpu_dmma_peak(ctypes.byref(t)), "patgpu_dmma_peak")
+    return t.value
 
 
 def rys_host(n: int, T: float):

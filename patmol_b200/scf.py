@@ -47,6 +47,7 @@ class RHFResult:
     converged: bool
     enuc: float
     quartets_computed: list | None = None   # per iteration, incremental builds
+    fock_seconds: float = 0.0              # device-timed Fock builds of the iterations
 
 
 def orthogonalizer(S: np.ndarray, smin: float = 1e-10) -> np.ndarray:
@@ -60,13 +61,13 @@ class _RHFState:
     """One molecule's closed-shell iteration (host side of rhf_scf_update)."""
 
     def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float, device_linalg: bool = False,
-                 comm_tol: float = 1e-9, dp_tol: float = 1e-8):
+                 comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10):
         if basis.nelec % 2 or basis.mult != 1:
             raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
         self.n = basis.norb
         self.nocc = basis.nelec // 2
         self.S, self.H = unpack(Sp, self.n), unpack(Hp, self.n)
-        self.X = orthogonalizer(self.S)
+        self.X = orthogonalizer(self.S, smin)
         self.enuc = nuclear_repulsion(basis)
         self.ndiis, self.conv = ndiis, conv
         self.comm_tol, self.dp_tol = comm_tol, dp_tol
@@ -192,7 +193,7 @@ class IncrementalFock:
 def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
         maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
         tau_inc: float = 1e-14, device_linalg: bool = False, tau_fp32: float = 0.0, tau_inc32: float = 0.0,
-        comm_tol: float = 1e-9, dp_tol: float = 1e-8) -> RHFResult:
+        comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10) -> RHFResult:
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
     from a full build.  device_linalg=True diagonalises on the GPU.
@@ -202,13 +203,18 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
     Sp, Hp = _setup(gb, dpm)
     if tau_fp32 > 0.0:
         gb.set_mixed_precision(tau_fp32)
-    st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg, comm_tol=comm_tol, dp_tol=dp_tol)
+    st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg, comm_tol=comm_tol, dp_tol=dp_tol,
+                   smin=smin)
     fock = IncrementalFock(gb, tau_inc, tau32=tau_inc32) if incremental else None
+    fock_ns = 0.0
     while st.it < maxit and not st.converged:
         Pp = st.packed_density()
-        st.step(fock(Pp) if fock else gb.rhf_form_gmatrix(Pp))
+        G = fock(Pp) if fock else gb.rhf_form_gmatrix(Pp)
+        fock_ns += gb.last_timing()[0]
+        st.step(G)
     res = st.finish(gb.rhf_form_gmatrix(st.packed_density()))
     res.quartets_computed = fock.computed if fock else None
+    res.fock_seconds = fock_ns * 1e-9
     if tau_fp32 > 0.0:
         gb.set_mixed_precision(0.0)
     if gpu is None:
@@ -219,7 +225,8 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
 def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-12, maxit: int = 100,
               schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False, tau_inc: float = 1e-11,
               tau_inc32: float = 0.0, fp32_dp_min: float = 1e-4, full_every: int = 8, comm_tol: float = 1e-9,
-              dp_tol: float = 1e-8, computed: list | None = None):
+              dp_tol: float = 1e-8, computed: list | None = None, smin: float = 1e-10,
+              device_linalg: bool = False, fock_seconds: list | None = None):
     """Closed-shell SCF of many molecules in lock step: every iteration is one
     batched Fock build (one CUDA graph over all molecules, patgpu_batch_*),
     then each molecule's host step.  Converged molecules keep their density.
@@ -231,12 +238,14 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
     than fp32_dp_min, tau_inc32 > 0 also runs its kept quartets with a
     density-weighted bound below tau_inc32 in FP32 (the difference builds of
     the final iterations stay FP64).  The final energies come from a full
-    build.  computed, if given, receives the quartets of every build."""
+    build.  computed, if given, receives the quartets of every build, and
+    fock_seconds the device-timed seconds of every batched build."""
     gbs = [GpuBasis(b, schwarz_tau=schwarz_tau) for b in bases]
     states = []
     for b, gb in zip(bases, gbs):
         Sp, Hp = _setup(gb, dpm)
-        states.append(_RHFState(b, Sp, Hp, ndiis, conv, comm_tol=comm_tol, dp_tol=dp_tol))
+        states.append(_RHFState(b, Sp, Hp, ndiis, conv, comm_tol=comm_tol, dp_tol=dp_tol, smin=smin,
+                                device_linalg=device_linalg))
     batch = GpuBatch(gbs)
     if tau_fp32 > 0.0:
         batch.set_mixed_precision(tau_fp32)
@@ -255,6 +264,8 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
             Gs = [Gp + dG for Gp, dG in zip(Gprev, batch.rhf_form_gmatrix(dPs))]
         if computed is not None:
             computed.append(batch.last_computed())
+        if fock_seconds is not None:
+            fock_seconds.append(batch.last_timing_ns() * 1e-9)
         Gprev, Pprev = Gs, Ps
         for st, G in zip(states, Gs):
             if not st.converged:
