@@ -1,7 +1,8 @@
 """Generate the golden fixtures of tests/golden from the compiled reference.
 
 Run in the build container (it needs the reference tree to build
-oracle/_ref):  python tests/golden/make_golden.py
+oracle/_ref):
+    PATMOL_REFERENCE=<reference tree> python tests/golden/make_golden.py
 Every number stored here comes from the reference's own code
 (oracle/_ref/ref_harness, oracle/_ref/ref_rysdump) run on seeded inputs, or
 from the reference's shipped SF6 fixture (patin.dat, short.gs.dat).
@@ -24,7 +25,7 @@ from patmol_b200.basis import Basis  # noqa: E402
 import patref  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = os.environ.get("PATMOL_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("PATMOL_REFERENCE", "")
 
 
 def mini_basis() -> Basis:
@@ -55,6 +56,8 @@ def seeded_density(n: int, seed: int) -> np.ndarray:
 
 
 def main():
+    if not REFERENCE:
+        raise SystemExit("set PATMOL_REFERENCE to the reference source tree")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REFERENCE}"], check=True)
     meta = {}
 
