@@ -66,6 +66,12 @@ def parse():
                     help="molecules of the SCF-iteration leg (config-3 recipe); 0 skips it")
     ap.add_argument("--scf-max-atoms", type=int, default=24,
                     help="molecule sizes of the SCF-iteration leg are uniform in 3..this")
+    ap.add_argument("--scf-level-shift", type=float, default=0.3,
+                    help="SCF-iteration leg: virtual level shift (Eh) while the DIIS error exceeds 1e-3")
+    ap.add_argument("--scf-full-every", type=int, default=8,
+                    help="SCF-iteration leg: full Fock build every this many iterations of the mixed batch")
+    ap.add_argument("--scf-tau-full", type=float, default=1e-14,
+                    help="SCF-iteration leg: density screening of the mixed batch's full builds (0: none)")
     ap.add_argument("--no-organic40", action="store_true", help="skip the 40-atom (config-2) leg")
     ap.add_argument("--scf-iters", type=int, default=3,
                     help="alkane_dpm: SCF iterations before the gradient (timing; the converged "
@@ -280,7 +286,8 @@ def scf_iteration_leg(a, torch):
     rng = np.random.default_rng(303)
     sizes = rng.integers(3, a.scf_max_atoms + 1, size=a.scf_molecules)
     bases = [configs.organic_basis(int(k), 3000 + i, with_f=False) for i, k in enumerate(sizes)]
-    kw = dict(conv=1e-10, comm_tol=1e-6, dp_tol=1e-6, maxit=80, smin=1e-7, device_linalg=True)
+    kw = dict(conv=1e-10, comm_tol=1e-6, dp_tol=1e-6, maxit=100, smin=1e-7, device_linalg=True,
+              level_shift=a.scf_level_shift, shift_tol=1e-3)
     torch.cuda.synchronize()
     t0 = time.time()
     plain = [scf.rhf(b, **kw) for b in bases]
@@ -290,7 +297,8 @@ def scf_iteration_leg(a, torch):
     computed, fock_b = [], []
     t0 = time.time()
     mixed = scf.rhf_batch(bases, tau_fp32=a.tau_fp32, incremental=True, tau_inc=1e-10, tau_inc32=1e-6,
-                          computed=computed, fock_seconds=fock_b, **kw)
+                          full_every=a.scf_full_every, tau_full=a.scf_tau_full, computed=computed,
+                          fock_seconds=fock_b, **kw)
     t_mixed = time.time() - t0
     it_mixed = sum(r.iterations for r in mixed)
     fock_mixed = sum(fock_b)
@@ -301,13 +309,19 @@ def scf_iteration_leg(a, torch):
             "plain_fp64": {"wall_s": t_plain, "fock_s": fock_plain, "iterations": it_plain,
                            "fock_s_per_scf_iteration": fock_plain / it_plain,
                            "wall_s_per_scf_iteration": t_plain / it_plain,
-                           "converged": int(sum(r.converged for r in plain))},
+                           "converged": int(sum(r.converged for r in plain)),
+                           "iterations_per_molecule": [r.iterations for r in plain],
+                           "fock_s_per_molecule": [r.fock_seconds for r in plain]},
             "mixed_batched": {"wall_s": t_mixed, "fock_s": fock_mixed, "iterations": it_mixed,
                               "fock_s_per_scf_iteration": fock_mixed / it_mixed,
                               "wall_s_per_scf_iteration": t_mixed / it_mixed,
                               "converged": int(sum(r.converged for r in mixed)), "tau_fp32": a.tau_fp32,
-                              "tau_inc": 1e-10, "tau_inc32": 1e-6, "lockstep_iterations": len(computed),
-                              "quartets_per_build": computed},
+                              "tau_inc": 1e-10, "tau_inc32": 1e-6, "full_every": a.scf_full_every,
+                              "tau_full": a.scf_tau_full, "lockstep_iterations": len(computed),
+                              "iterations_per_molecule": [r.iterations for r in mixed],
+                              "quartets_per_build": computed, "fock_s_per_build": fock_b},
+            "level_shift": a.scf_level_shift,
+            "energies_plain": [r.energy for r in plain],
             "scf_iteration_speedup_fock": (it_mixed / fock_mixed) / (it_plain / fock_plain),
             "scf_iteration_speedup_wall": (it_mixed / t_mixed) / (it_plain / t_plain),
             "max_abs_dE": max(dE), "dE_per_molecule": dE}

@@ -29,6 +29,24 @@ inline bool first_on_device(unsigned long long *mask)
     const unsigned long long bit = 1ull << (dev & 63);
     return !(__atomic_fetch_or(mask, bit, __ATOMIC_ACQ_REL) & bit);
 }
+
+// Blocks of `func` (block threads, smem dynamic bytes) that one SM holds at
+// once, from the occupancy calculator, cached per device in cache[64] (0 =
+// not yet asked).  The class kernels loop grid-stride over their quartets,
+// so a grid of this many blocks per SM runs as one wave: no partial last
+// wave leaves SMs idle at the end of a launch.
+inline int resident_blocks(const void *func, int block, size_t smem, int *cache)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    dev &= 63;
+    int v = __atomic_load_n(cache + dev, __ATOMIC_ACQUIRE);
+    if (v > 0) return v;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, func, block, smem) != cudaSuccess || occ < 1) occ = 1;
+    __atomic_store_n(cache + dev, occ, __ATOMIC_RELEASE);
+    return occ;
+}
 #endif
 
 // Cartesian exponents in the order of basis.c:294-308: lx descending, then
@@ -75,8 +93,14 @@ struct RysConst {
 // Evaluate function f (0..n-1: node x = t^2, n..2n-1: weight) of the
 // n-root Rys rule at T.  Chebyshev series (Clenshaw) on unit intervals
 // below tmax[n], generalised-Laguerre limit above.
+// Coefficient layouts, per n from rc.off[n] and per interval k a block of
+// 2n (deg+1) doubles: series-major, coefficient j of function f at
+// f (deg+1) + j (rys_table.h as generated, interleaved = false), or
+// coefficient-major at j 2n + f (interleaved = true: the copy on the
+// device, where the lanes evaluating one quartet's 2n series read
+// neighbouring words at every step).
 PG_HD double rys_eval(int n, int f, double T, const RysConst &rc, const double *__restrict__ coef,
-                      int deg)
+                      int deg, bool interleaved = false)
 {
     if (!(T < (double)rc.tmax[n])) {   // also takes NaN: no table access
         if (f < n) return rc.lag_x[n][f] / T;
@@ -84,13 +108,15 @@ PG_HD double rys_eval(int n, int f, double T, const RysConst &rc, const double *
     }
     int k = (int)T;
     double u = 2.0 * (T - (double)k) - 1.0;
-    const double *c = coef + rc.off[n] + ((size_t)k * 2 * n + f) * (deg + 1);
+    const size_t blk = rc.off[n] + (size_t)k * 2 * n * (deg + 1);
+    const double *c = coef + blk + (interleaved ? (size_t)f : (size_t)f * (deg + 1));
+    const int cs = interleaved ? 2 * n : 1;
     double b1 = 0.0, b2 = 0.0, u2 = 2.0 * u;
     for (int j = deg; j >= 1; --j) {
 #ifdef __CUDA_ARCH__
-        double cj = __ldg(c + j);
+        double cj = __ldg(c + j * cs);
 #else
-        double cj = c[j];
+        double cj = c[j * cs];
 #endif
         double t = fma(u2, b1, cj - b2);
         b2 = b1;
@@ -102,6 +128,18 @@ PG_HD double rys_eval(int n, int f, double T, const RysConst &rc, const double *
     double c0 = c[0];
 #endif
     return fma(u, b1, c0 - b2);
+}
+
+// The coefficient-major copy of a series-major table (see rys_eval); nmax
+// functions sets, rc.off[nmax + 1] = total size.
+inline void rys_interleave(const double *src, double *dst, const int *off, const int *tmax, int nmax, int deg)
+{
+    for (int n = 1; n <= nmax; ++n)
+        for (int k = 0; k < tmax[n]; ++k) {
+            const size_t blk = off[n] + (size_t)k * 2 * n * (deg + 1);
+            for (int f = 0; f < 2 * n; ++f)
+                for (int j = 0; j <= deg; ++j) dst[blk + (size_t)j * 2 * n + f] = src[blk + (size_t)f * (deg + 1) + j];
+        }
 }
 
 // ---------------------------------------------------------------- Boys

@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kBlk, 4) eri_grad_kernel(const EriArgs args, c
                     pqx = Px - Qx; pqy = Py - Qy; pqz = Pz - Qz;
                     const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
                     for (int f = lane; f < 2 * NR; f += TQ)
-                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDegG);
+                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDegG, true);
                 }
             }
             __syncthreads();

@@ -301,7 +301,7 @@ eri_class_kernel(const EriArgs args)
                     pqx = Px - Qx; pqy = Py - Qy; pqz = Pz - Qz;
                     const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
                     for (int f = lane; f < 2 * NR; f += TQ)
-                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg);
+                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg, true);
                 }
             }
             __syncthreads();
@@ -528,8 +528,10 @@ cudaError_t launch_one(const EriArgs &a, cudaStream_t stream, int num_sms)
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
     }
+    static int resident[64] = {};
     long long blocks = (a.nquart + S::NTEAM - 1) / S::NTEAM;
-    long long cap = (long long)num_sms * 32;
+    const long long cap = (long long)num_sms *
+        resident_blocks((const void *)eri_class_kernel<LA, LB, LC, LD, NDEN, R>, S::BLK, S::SMEM, resident);
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
     eri_class_kernel<LA, LB, LC, LD, NDEN, R><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);

@@ -112,8 +112,8 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
                 const double T = p * qx / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
 #pragma unroll 1
                 for (int r = 0; r < NR; ++r) {
-                    const double x = rys_eval(NR, r, T, c_rys, args.rys_coef, kRysDeg);
-                    const double w = rys_eval(NR, NR + r, T, c_rys, args.rys_coef, kRysDeg);
+                    const double x = rys_eval(NR, r, T, c_rys, args.rys_coef, kRysDeg, true);
+                    const double w = rys_eval(NR, NR + r, T, c_rys, args.rys_coef, kRysDeg, true);
                     const double f = x / ppq, B00 = 0.5 * f;
                     const double B10 = (0.5 - B00 * qx) / p, B01 = (0.5 - B00 * p) / qx;
                     double tx[TSZ], ty[TSZ], tz[TSZ];
@@ -246,8 +246,10 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
 template <int LA, int LB, int LC, int LD, int NDEN>
 cudaError_t launch_reg(const EriArgs &a, cudaStream_t stream, int num_sms)
 {
+    static int resident[64] = {};
     long long blocks = (a.nquart + 127) / 128;
-    long long cap = (long long)num_sms * 16;
+    const long long cap =
+        (long long)num_sms * resident_blocks((const void *)eri_reg_kernel<LA, LB, LC, LD, NDEN>, 128, 0, resident);
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
     eri_reg_kernel<LA, LB, LC, LD, NDEN><<<(unsigned)blocks, 128, 0, stream>>>(a);

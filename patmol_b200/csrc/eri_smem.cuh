@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(128, MINB) eri_smem_kernel(const EriArgs args)
                     pqx = Px - Qx; pqy = Py - Qy; pqz = Pz - Qz;
                     const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
                     for (int f = lane; f < 2 * NR; f += TQ)
-                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg);
+                        s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg, true);
                 }
             }
             __syncthreads();
@@ -338,8 +338,10 @@ cudaError_t launch_smem(const EriArgs &a, cudaStream_t stream, int num_sms)
                                      cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
     }
+    static int resident[64] = {};
     long long blocks = (a.nquart + S::NTEAM - 1) / S::NTEAM;
-    long long cap = (long long)num_sms * 16;
+    const long long cap = (long long)num_sms *
+        resident_blocks((const void *)eri_smem_kernel<LA, LB, LC, LD, R, MINB>, S::BLK, S::SMEM, resident);
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
     eri_smem_kernel<LA, LB, LC, LD, R, MINB><<<(unsigned)blocks, S::BLK, S::SMEM, stream>>>(a);

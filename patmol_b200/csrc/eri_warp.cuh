@@ -63,14 +63,25 @@ struct WarpShape {
     static constexpr int OBD = NAB, OBC = OBD + NB * ND, OAD = OBC + NB * NC, OAC = OAD + NA * ND;
     static constexpr int NDB = OAC + NA * NC;
     static constexpr int PS = 2 * NA + 2 * NB;              // exchange partials per lane and set
+    // Shared-memory strides, chosen against bank conflicts.  Each lane's
+    // recursion job writes one table of TSZ entries and each lane stores its
+    // PS exchange partials; the lanes of a warp store at the same offset in
+    // their own table (partial block) at once.  With odd strides TST and PSP
+    // (in R and double words) and a team stride TEAM congruent to NL*TST
+    // modulo 16 doubles, the 16 lanes of a half warp (one wavefront of 64-bit
+    // accesses) hit 16 distinct bank pairs.  PSP is also congruent to TST
+    // modulo 16, so one team stride serves both stores.
+    static constexpr int TST = TSZ | 1;
+    static constexpr int PSP = PS + (((TST - PS) % 16) + 16) % 16;
     // per-team shared memory, in doubles: roots/weights, staged densities,
     // tables (later the exchange partials), one chunk's J(ab) partials
     static constexpr int RW = 2 * NR;
-    static constexpr int TABD = (3 * NR * TSZ * (int)sizeof(R) + 7) / 8;
-    static constexpr int PART = NL > 1 ? NL * PS * NDEN : 0;
+    static constexpr int TABD = (3 * NR * TST * (int)sizeof(R) + 7) / 8;
+    static constexpr int PART = NL > 1 ? NL * PSP * NDEN : 0;
     static constexpr int REGION = TABD > PART ? TABD : PART;
     static constexpr int WCH = NL > 1 ? CH * NL : 0;
-    static constexpr int TEAM = RW + NDB * NDEN + REGION + WCH;
+    static constexpr int TEAM0 = RW + NDB * NDEN + REGION + WCH;
+    static constexpr int TEAM = sizeof(R) == 8 ? TEAM0 + (((NL * TST - TEAM0) % 16) + 16) % 16 : TEAM0;
     // teams per warp: 32/NL, fewer where the teams' shared memory would pass
     // 28 KB a warp (the large-bra classes with one or three ket lanes), so
     // that an SM still holds 8 or more warps
@@ -89,8 +100,8 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
 {
     using S = WarpShape<LA, LB, LC, LD, NDEN, R>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NAB = S::NAB;
-    constexpr int NR = S::NR, TAB = S::TAB, TSZ = S::TSZ, NL = S::NL, Q = S::Q;
-    constexpr int NCH = S::NCH, CH = S::CH, NDB = S::NDB, PS = S::PS;
+    constexpr int NR = S::NR, TAB = S::TAB, TST = S::TST, NL = S::NL, Q = S::Q;
+    constexpr int NCH = S::NCH, CH = S::CH, NDB = S::NDB, PSP = S::PSP;
     extern __shared__ double smem[];
 
     const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
@@ -153,7 +164,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                 qcx = Qx - k3.x; qcy = Qy - k3.y; qcz = Qz - k4.x;
                 pqx = Px - Qx; pqy = Py - Qy; pqz = Pz - Qz;
                 const double T = p * q / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
-                for (int f = lt; f < 2 * NR; f += NL) s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg);
+                for (int f = lt; f < 2 * NR; f += NL) s_rw[f] = rys_eval(NR, f, T, c_rys, args.rys_coef, kRysDeg, true);
             }
             // stage D(ab) (every lane reads all of it), and with the exchange
             // densities kept in shared memory also D(bd), D(bc), D(ad), D(ac);
@@ -198,7 +209,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                 const double pq = dim == 0 ? pqx : (dim == 1 ? pqy : pqz);
                 const double ab = dim == 0 ? abx : (dim == 1 ? aby : abz);
                 const double cd = dim == 0 ? cdx : (dim == 1 ? cdy : cdz);
-                R *tab = reinterpret_cast<R *>(s_tab) + (dim * NR + r) * TSZ;
+                R *tab = reinterpret_cast<R *>(s_tab) + (dim * NR + r) * TST;
                 if constexpr (S::NSPLIT == 1) {
                     vrr_hrr<LA, LB, LC, LD, R>(tab, R(dim == 2 ? w * sr : 1.0), R(B00), R(B10), R(B01),
                                                R(pa - q * pq * f), R(qc + p * pq * f), R(ab), R(cd));
@@ -256,8 +267,8 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
         }
         const R *tb = reinterpret_cast<const R *>(s_tab);
         const R *X = tb + tcdx * TAB;
-        const R *Y = tb + NR * TSZ + tcdy * TAB;
-        const R *Z = tb + 2 * NR * TSZ + tcdz * TAB;
+        const R *Y = tb + NR * TST + tcdy * TAB;
+        const R *Z = tb + 2 * NR * TST + tcdz * TAB;
         auto chunk = [&](auto cst) {
             constexpr int c = decltype(cst)::value;
             constexpr int CHN = (c + 1) * CH <= NAB ? CH : NAB - c * CH;
@@ -265,7 +276,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
 #pragma unroll
             for (int j = 0; j < CH; ++j) acc[j] = R(0);
             if (work) {
-                assemble<LA, LB, NR, TSZ, c * CH, CH>(acc, X, Y, Z);
+                assemble<LA, LB, NR, TST, c * CH, CH>(acc, X, Y, Z);
 #pragma unroll
                 for (int j = 0; j < CHN; ++j) {
                     const int ab = c * CH + j;
@@ -349,7 +360,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
             if (work) {
 #pragma unroll
                 for (int s = 0; s < NDEN; ++s) {
-                    double *pp = s_part + ((size_t)s * NL + lt) * PS;
+                    double *pp = s_part + ((size_t)s * NL + lt) * PSP;
 #pragma unroll
                     for (int a = 0; a < NA; ++a) { pp[a] = Pac[s][a]; pp[NA + a] = Pad[s][a]; }
 #pragma unroll
@@ -365,12 +376,12 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                 for (int s = 0; s < NDEN; ++s) {
                     double *A = mode == MODE_JK ? args.A1 : (s == 0 ? args.A0 : args.A1);
                     const double sg = mode == MODE_JK ? sK : -sK;
-                    const double *pp = s_part + (size_t)s * NL * PS;
+                    const double *pp = s_part + (size_t)s * NL * PSP;
                     for (int t = lt; t < NA * NC; t += NL) {
                         const int a = t / NC, c = t - (t / NC) * NC;
                         double sum = 0.0;
 #pragma unroll
-                        for (int d = 0; d < ND; ++d) sum += pp[(c * ND + d) * PS + a];
+                        for (int d = 0; d < ND; ++d) sum += pp[(c * ND + d) * PSP + a];
                         acc_add(A, (size_t)(fa + a) * n + fc + c, sg * c_norm[LA][a] * c_norm[LC][c] * sum, args.det,
                                 args.err);
                     }
@@ -378,7 +389,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                         const int a = t / ND, d = t - (t / ND) * ND;
                         double sum = 0.0;
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) sum += pp[(c * ND + d) * PS + NA + a];
+                        for (int c = 0; c < NC; ++c) sum += pp[(c * ND + d) * PSP + NA + a];
                         acc_add(A, (size_t)(fa + a) * n + fd + d, sg * c_norm[LA][a] * c_norm[LD][d] * sum, args.det,
                                 args.err);
                     }
@@ -386,7 +397,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                         const int b = t / NC, c = t - (t / NC) * NC;
                         double sum = 0.0;
 #pragma unroll
-                        for (int d = 0; d < ND; ++d) sum += pp[(c * ND + d) * PS + 2 * NA + b];
+                        for (int d = 0; d < ND; ++d) sum += pp[(c * ND + d) * PSP + 2 * NA + b];
                         acc_add(A, (size_t)(fb + b) * n + fc + c, sg * c_norm[LB][b] * c_norm[LC][c] * sum, args.det,
                                 args.err);
                     }
@@ -394,7 +405,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                         const int b = t / ND, d = t - (t / ND) * ND;
                         double sum = 0.0;
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) sum += pp[(c * ND + d) * PS + 2 * NA + NB + b];
+                        for (int c = 0; c < NC; ++c) sum += pp[(c * ND + d) * PSP + 2 * NA + NB + b];
                         acc_add(A, (size_t)(fb + b) * n + fd + d, sg * c_norm[LB][b] * c_norm[LD][d] * sum, args.det,
                                 args.err);
                     }
@@ -416,9 +427,11 @@ cudaError_t launch_warp(const EriArgs &a, cudaStream_t stream, int num_sms)
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
     }
+    static int resident[64] = {};
     const long long per_block = (long long)S::Q * S::WARPS;
     long long blocks = (a.nquart + per_block - 1) / per_block;
-    const long long cap = (long long)num_sms * 16;
+    const long long cap = (long long)num_sms * resident_blocks((const void *)eri_warp_kernel<LA, LB, LC, LD, NDEN, R>,
+                                                               32 * S::WARPS, S::SMEM, resident);
     if (blocks > cap) blocks = cap;
     if (blocks < 1) return cudaSuccess;
     eri_warp_kernel<LA, LB, LC, LD, NDEN, R><<<(unsigned)blocks, 32 * S::WARPS, S::SMEM, stream>>>(a);

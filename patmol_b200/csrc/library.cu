@@ -104,9 +104,12 @@ static int init_tables()
     std::lock_guard<std::mutex> g(g_tab_lock);
     if (g_tab_state[dev] == 0) {
         auto *b = new DBuf();
+        // the device keeps the coefficient-major copy (rys_eval, interleaved)
+        std::vector<double> il(rys_ncoef);
+        rys_interleave(rys_coef_host, il.data(), rys_off, rys_tmax, RYS_NMAX, RYS_DEG);
         const bool ok =
             b->ensure(sizeof(double) * rys_ncoef) == cudaSuccess &&
-            cudaMemcpy(b->p, rys_coef_host, sizeof(double) * rys_ncoef, cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(b->p, il.data(), sizeof(double) * rys_ncoef, cudaMemcpyHostToDevice) == cudaSuccess &&
             upload_rys_constants(host_rys_const()) == cudaSuccess && upload_onebody_constants() == cudaSuccess;
         g_rys_coef[dev] = b;
         g_tab_state[dev] = ok ? 1 : -1;
@@ -493,17 +496,66 @@ __global__ void count_kernel(const EriArgs a, unsigned long long *cnt)
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, c);
 }
 
+// Which quartets may run in FP32.  The Schwarz bound Q_ab Q_cd limits an
+// integral, not the terms the Rys scheme sums to get it: for diffuse
+// distributions far apart the roots' terms are many orders of magnitude
+// larger than their sum (the sum is a high multipole; each term carries
+// powers of the root-scaled P-Q distance), and FP32 rounding errors scale
+// with the terms.  term_bound is an upper estimate of those terms for bra
+// pair u and ket pair v of a class with la+lb = lab and lc+ld = lcd: per
+// primitive pair, the prefactor 2 pi^(5/2) |K_ab K_cd| / sqrt(p+q) times
+// (2|A-B| + q/(p+q)|P-Q| + sqrt((lab+1)/2p))^lab (every recursion and
+// transfer entry of the bra side stays below this power; likewise the ket
+// side), summed over primitive pairs.  The FP32 window is term_bound <
+// tau_fp32, which keeps FP32 rounding near eps_32 * tau_fp32 per integral.
+// Contracted pairs with more than 64 primitive-pair combinations stay FP64.
+constexpr double kTermSR = 34.98683665524972497;   // 2 pi^(5/2)
+
+__device__ double ipow_small(double x, int l)
+{
+    double r = 1.0;
+    for (int i = 0; i < l; ++i) r *= x;
+    return r;
+}
+
+__device__ double term_bound(const EriArgs &a, int u, int v, int lab, int lcd)
+{
+    const int pu = a.pr.pstart[u], nu = a.pr.pnum[u], pv = a.pr.pstart[v], nv = a.pr.pnum[v];
+    if (nu * nv > 64) return INFINITY;
+    const double abl = sqrt(a.pr.abx[u] * a.pr.abx[u] + a.pr.aby[u] * a.pr.aby[u] + a.pr.abz[u] * a.pr.abz[u]);
+    const double cdl = sqrt(a.pr.abx[v] * a.pr.abx[v] + a.pr.aby[v] * a.pr.aby[v] + a.pr.abz[v] * a.pr.abz[v]);
+    double e = 0.0;
+    for (int ib = pu; ib < pu + nu; ++ib)
+        for (int ik = pv; ik < pv + nv; ++ik) {
+            const double p = a.pp.p[ib], q = a.pp.p[ik], ppq = p + q;
+            const double dx = a.pp.px[ib] - a.pp.px[ik], dy = a.pp.py[ib] - a.pp.py[ik],
+                         dz = a.pp.pz[ib] - a.pp.pz[ik];
+            const double R = sqrt(dx * dx + dy * dy + dz * dz);
+            const double sb = 2.0 * abl + q / ppq * R + sqrt((lab + 1) / (2.0 * p));
+            const double sk = 2.0 * cdl + p / ppq * R + sqrt((lcd + 1) / (2.0 * q));
+            e += kTermSR * fabs(a.pp.K[ib] * a.pp.K[ik]) * rsqrt(ppq) * ipow_small(sb, lab) * ipow_small(sk, lcd);
+        }
+    return e == e ? e : INFINITY;
+}
+
 // Stream compaction of one window of a class's implicit quartet space: the
 // (bra pair, ket pair) of every surviving item, packed as u | v << 32 and
 // appended at out[*cursor++] with
-// warp-aggregated atomics (order within a warp kept).
-__global__ void compact_kernel(const EriArgs a, unsigned long long *out, unsigned long long *cursor)
+// warp-aggregated atomics (order within a warp kept).  With lab >= 0 an
+// item is kept only when its term_bound lies in [elo, ehi) as well (the
+// FP64 or the FP32 window of mixed precision).
+__global__ void compact_kernel(const EriArgs a, unsigned long long *out, unsigned long long *cursor, int lab = -1,
+                               int lcd = 0, double elo = 0.0, double ehi = 0.0)
 {
     for (long long qi0 = (long long)blockIdx.x * blockDim.x; qi0 < a.nquart;
          qi0 += (long long)gridDim.x * blockDim.x) {
         const long long qi = qi0 + threadIdx.x;
         int u, v;
-        const bool keep = qi < a.nquart && eri_quartet_at(a, qi, u, v);
+        bool keep = qi < a.nquart && eri_quartet_at(a, qi, u, v);
+        if (keep && lab >= 0) {
+            const double e = term_bound(a, u, v, lab, lcd);
+            keep = e >= elo && e < ehi;
+        }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (!m) continue;
         const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
@@ -554,10 +606,15 @@ static int build_lists(patgpu_basis *h)
     unsigned long long *out = h->d_list.as<unsigned long long>();
     for (size_t k = 0; k < h->work.size(); ++k) {
         const ClassWork &w = h->work[k];
-        // FP64 window first, then the FP32 window behind it
-        EriArgs a = class_args(h, w, MODE_RHF, mixed ? h->tau_mix : lo, INFINITY);
+        // FP64 window first (term_bound >= tau_mix), then the FP32 window
+        // behind it; both screened by the Schwarz bound at tau
+        EriArgs a = class_args(h, w, MODE_RHF, lo, INFINITY);
         const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
-        compact_kernel<<<std::max(g, 1), 256, 0, h->stream>>>(a, out + w.loff, dcur.as<unsigned long long>() + 2 * k);
+        if (mixed)
+            compact_kernel<<<std::max(g, 1), 256, 0, h->stream>>>(a, out + w.loff, dcur.as<unsigned long long>() + 2 * k,
+                                                                  w.la + w.lb, w.lc + w.ld, h->tau_mix, INFINITY);
+        else
+            compact_kernel<<<std::max(g, 1), 256, 0, h->stream>>>(a, out + w.loff, dcur.as<unsigned long long>() + 2 * k);
     }
     PG_CUDA(cudaGetLastError());
     std::vector<unsigned long long> cur(std::max<size_t>(nc, 1), 0);
@@ -568,10 +625,11 @@ static int build_lists(patgpu_basis *h)
     if (mixed) {
         for (size_t k = 0; k < h->work.size(); ++k) {
             const ClassWork &w = h->work[k];
-            EriArgs a = class_args(h, w, MODE_RHF, lo, h->tau_mix);
+            EriArgs a = class_args(h, w, MODE_RHF, lo, INFINITY);
             const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
             compact_kernel<<<std::max(g, 1), 256, 0, h->stream>>>(a, out + w.loff + w.nhi,
-                                                                  dcur.as<unsigned long long>() + 2 * k + 1);
+                                                                  dcur.as<unsigned long long>() + 2 * k + 1,
+                                                                  w.la + w.lb, w.lc + w.ld, -1.0, h->tau_mix);
         }
         PG_CUDA(cudaGetLastError());
         PG_CUDA(cudaMemcpyAsync(cur.data(), dcur.p, sizeof(unsigned long long) * cur.size(), cudaMemcpyDeviceToHost,
@@ -669,9 +727,32 @@ static std::tuple<int, int, int, int, int> tune_key(const patgpu_basis *h, const
                            w.count >= 8192 ? 1 : 0, kind);
 }
 
+// PATGPU_TUNE_SAVE=<file> appends every choice the tuner makes to <file>;
+// PATGPU_TUNE_LOAD=<file> seeds the process's choices from such a file
+// before the first tuning, so that a second run (a profiler's, whose own
+// launch overhead would distort the timings) launches the same kernels as
+// the run that wrote it.  Lines: device class primitive-structure size kind
+// variant.
+static bool g_tune_loaded = false;
+
+static void tune_load_locked()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char *path = getenv("PATGPU_TUNE_LOAD");
+    if (!path) return;
+    FILE *f = fopen(path, "r");
+    if (!f) return;
+    int d, c, sp, big, kind, var;
+    while (fscanf(f, "%d %d %d %d %d %d", &d, &c, &sp, &big, &kind, &var) == 6)
+        g_tune_cache[std::make_tuple(d, c, sp, big, kind)] = var;
+    fclose(f);
+}
+
 static bool tune_cached(const patgpu_basis *h, const ClassWork &w, int kind, int *variant)
 {
     std::lock_guard<std::mutex> g(g_tune_lock);
+    tune_load_locked();
     auto it = g_tune_cache.find(tune_key(h, w, kind));
     if (it == g_tune_cache.end()) return false;
     *variant = it->second;
@@ -681,7 +762,15 @@ static bool tune_cached(const patgpu_basis *h, const ClassWork &w, int kind, int
 static void tune_store(const patgpu_basis *h, const ClassWork &w, int kind, int variant)
 {
     std::lock_guard<std::mutex> g(g_tune_lock);
-    g_tune_cache[tune_key(h, w, kind)] = variant;
+    const auto key = tune_key(h, w, kind);
+    g_tune_cache[key] = variant;
+    if (const char *path = getenv("PATGPU_TUNE_SAVE")) {
+        if (FILE *f = fopen(path, "a")) {
+            fprintf(f, "%d %d %d %d %d %d\n", std::get<0>(key), std::get<1>(key), std::get<2>(key), std::get<3>(key),
+                    std::get<4>(key), variant);
+            fclose(f);
+        }
+    }
 }
 
 static int tune_variants(patgpu_basis *h)
@@ -1010,11 +1099,12 @@ __device__ __forceinline__ void warp_append(bool keep, unsigned long long v, uns
 // Keep the list entries whose contribution bound Q_ab Q_cd max(4|D_ab|,
 // 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|) reaches tau (shell-block maxima;
 // the factor 4 covers the Coulomb weight).  A kept entry goes to the FP32
-// sublist (written downward from end32) when all32 is set (the Schwarz FP32
-// window) or its bound is below tau32, else to the FP64 sublist (upward from
-// out64); counts in cnt[0] and cnt[1].
+// sublist (written downward from end32) when all32 is set (the FP32 window
+// of mixed precision) or its density-weighted term bound (term_bound of the
+// class lab, lcd times the same density maximum) is below tau32, else to the
+// FP64 sublist (upward from out64); counts in cnt[0] and cnt[1].
 __global__ void density_filter_kernel(const EriArgs a, const double *__restrict__ dsh, int nsh, double tau,
-                                      double tau32, int all32, unsigned long long *out64,
+                                      double tau32, int all32, int lab, int lcd, unsigned long long *out64,
                                       unsigned long long *end32, unsigned long long *cnt)
 {
     for (long long qi0 = (long long)blockIdx.x * blockDim.x; qi0 < a.nquart;
@@ -1027,9 +1117,9 @@ __global__ void density_filter_kernel(const EriArgs a, const double *__restrict_
             const int sa = a.pr.sa[u], sb = a.pr.sb[u], sc = a.pr.sa[v], sd = a.pr.sb[v];
             const double dj = 4.0 * fmax(dsh[sa * nsh + sb], dsh[sc * nsh + sd]);
             const double dk = fmax(fmax(dsh[sa * nsh + sc], dsh[sa * nsh + sd]), fmax(dsh[sb * nsh + sc], dsh[sb * nsh + sd]));
-            const double bound = a.Q[u] * a.Q[v] * fmax(dj, dk);
-            keep = bound >= tau;
-            low = all32 || bound < tau32;
+            const double dm = fmax(dj, dk);
+            keep = a.Q[u] * a.Q[v] * dm >= tau;
+            low = all32 || (keep && tau32 > 0.0 && term_bound(a, u, v, lab, lcd) * dm < tau32);
         }
         const unsigned long long k = qi < a.nquart ? a.klist[qi] : 0ull;
         warp_append(keep && !low, k, out64, cnt, false);
@@ -1058,7 +1148,7 @@ static int density_filter_enqueue(patgpu_basis *h, bool two, cudaStream_t s)
             if (a.nquart <= 0) continue;
             const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
             density_filter_kernel<<<std::max(g, 1), 256, 0, s>>>(
-                a, h->d_dsh.as<double>(), nsh, h->tau_dens, h->tau_dens32, win, out + w.loff,
+                a, h->d_dsh.as<double>(), nsh, h->tau_dens, h->tau_dens32, win, w.la + w.lb, w.lc + w.ld, out + w.loff,
                 out + w.loff + w.count, h->d_fcnt.as<unsigned long long>() + 2 * w.idx);
         }
     PG_CUDA(cudaGetLastError());
@@ -1759,26 +1849,11 @@ int patgpu_set_mixed_precision(patgpu_handle h, double tau_fp32)
     h->tau_mix = tau_fp32;
     h->nquart_fp32 = 0;
     if (tau_fp32 <= 0.0 || tau_fp32 <= h->tau) return h->lists ? build_lists(h) : 0;
-    DBuf dcnt;
-    PG_CUDA(dcnt.ensure(sizeof(unsigned long long)));
-    PG_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long), h->stream));
-    for (auto &w : h->work) {
-        EriArgs a = class_args(h, w, MODE_RHF, h->tau > 0.0 ? h->tau : -1.0, tau_fp32);
-        long long blocks = std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
-        count_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, h->stream>>>(a,
-                                                                                     dcnt.as<unsigned long long>());
-    }
-    PG_CUDA(cudaGetLastError());
-    unsigned long long c = 0;
-    PG_CUDA(cudaMemcpyAsync(&c, dcnt.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
-    PG_CUDA(cudaStreamSynchronize(h->stream));
-    h->nquart_fp32 = (long long)c;
+    // the lists split each class by term_bound (build_lists); mixed
+    // precision runs over the compacted lists only
     int rc = h->lists ? build_lists(h) : 0;
-    if (rc) return rc;
-    if (!h->lists) {   // mixed precision runs over the compacted lists only
-        h->nquart_fp32 = 0;
-        return 0;
-    }
+    if (rc || !h->lists) return rc;
+    for (const auto &w : h->work) h->nquart_fp32 += w.count - w.nhi;
     return tune_fp32(h);
 }
 

@@ -61,7 +61,8 @@ class _RHFState:
     """One molecule's closed-shell iteration (host side of rhf_scf_update)."""
 
     def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float, device_linalg: bool = False,
-                 comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10):
+                 comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10, level_shift: float = 0.0,
+                 shift_tol: float = 1e-3):
         if basis.nelec % 2 or basis.mult != 1:
             raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
         self.n = basis.norb
@@ -71,6 +72,9 @@ class _RHFState:
         self.enuc = nuclear_repulsion(basis)
         self.ndiis, self.conv = ndiis, conv
         self.comm_tol, self.dp_tol = comm_tol, dp_tol
+        # virtual-orbital level shift while the DIIS error is above shift_tol
+        self.level_shift, self.shift_tol = level_shift, shift_tol
+        self.err = np.inf
         # the step of rhf_scf_update after F (X^T F X, diagonalise, C, P) on the
         # GPU (patgpu_scf_*) or on the host
         self.linalg = GpuScfLinalg(self.X, self.nocc) if device_linalg else None
@@ -119,12 +123,19 @@ class _RHFState:
                 F = sum(ci * Fi for ci, Fi in zip(c, self.fs))
             except np.linalg.LinAlgError:
                 pass
+        self.err = float(np.max(np.abs(self.es[-1])))
+        if self.level_shift > 0.0 and self.err > self.shift_tol:
+            # F + s (S - S P S) raises the virtual space of the current
+            # orbitals by s (P S P = P): damps occupied-virtual rotations and
+            # orbital flips of small-gap molecules in the early iterations
+            SP = self.S @ self.P
+            F = F + self.level_shift * (self.S - SP @ self.S)
         self.eps, C, P_new = self.diag_density(F)
         dP = float(np.max(np.abs(P_new - self.P)))
         self.P = P_new
         self.dP = dP
         if self.e_old is not None and abs(energy - self.e_old) < self.conv and \
-                float(np.max(np.abs(self.es[-1]))) < self.comm_tol and dP < self.dp_tol:
+                self.err < self.comm_tol and dP < self.dp_tol:
             self.converged = True
         self.e_old = energy
 
@@ -193,19 +204,21 @@ class IncrementalFock:
 def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: float = 1e-12,
         maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
         tau_inc: float = 1e-14, device_linalg: bool = False, tau_fp32: float = 0.0, tau_inc32: float = 0.0,
-        comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10) -> RHFResult:
+        comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10, level_shift: float = 0.0,
+        shift_tol: float = 1e-3, full_every: int = 8) -> RHFResult:
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
     from a full build.  device_linalg=True diagonalises on the GPU.
     tau_fp32 > 0 runs quartets whose Schwarz bound is below it in FP32
-    (mixed precision) in every build."""
+    (mixed precision) in every build.  level_shift > 0 raises the virtual
+    orbitals by that many Eh while the DIIS error exceeds shift_tol."""
     gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
     Sp, Hp = _setup(gb, dpm)
     if tau_fp32 > 0.0:
         gb.set_mixed_precision(tau_fp32)
     st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg, comm_tol=comm_tol, dp_tol=dp_tol,
-                   smin=smin)
-    fock = IncrementalFock(gb, tau_inc, tau32=tau_inc32) if incremental else None
+                   smin=smin, level_shift=level_shift, shift_tol=shift_tol)
+    fock = IncrementalFock(gb, tau_inc, full_every=full_every, tau32=tau_inc32) if incremental else None
     fock_ns = 0.0
     while st.it < maxit and not st.converged:
         Pp = st.packed_density()
@@ -226,7 +239,8 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
               schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False, tau_inc: float = 1e-11,
               tau_inc32: float = 0.0, fp32_dp_min: float = 1e-4, full_every: int = 8, comm_tol: float = 1e-9,
               dp_tol: float = 1e-8, computed: list | None = None, smin: float = 1e-10,
-              device_linalg: bool = False, fock_seconds: list | None = None):
+              device_linalg: bool = False, fock_seconds: list | None = None, level_shift: float = 0.0,
+              shift_tol: float = 1e-3, tau_full: float = 0.0):
     """Closed-shell SCF of many molecules in lock step: every iteration is one
     batched Fock build (one CUDA graph over all molecules, patgpu_batch_*),
     then each molecule's host step.  Converged molecules keep their density.
@@ -237,15 +251,20 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
     it to the previous G; while a molecule's density still changes by more
     than fp32_dp_min, tau_inc32 > 0 also runs its kept quartets with a
     density-weighted bound below tau_inc32 in FP32 (the difference builds of
-    the final iterations stay FP64).  The final energies come from a full
-    build.  computed, if given, receives the quartets of every build, and
-    fock_seconds the device-timed seconds of every batched build."""
+    the final iterations stay FP64).  A converged molecule's difference is
+    zero, so the filter drops all of its quartets.  tau_full > 0 screens the
+    full builds of the iterations by the density as well, at that bound, and
+    gives converged molecules a zero density there, so that they cost
+    nothing after convergence.  The final energies come from an unscreened
+    full build.  level_shift / shift_tol as in rhf().  computed, if given,
+    receives the quartets of every build, and fock_seconds the device-timed
+    seconds of every batched build."""
     gbs = [GpuBasis(b, schwarz_tau=schwarz_tau) for b in bases]
     states = []
     for b, gb in zip(bases, gbs):
         Sp, Hp = _setup(gb, dpm)
         states.append(_RHFState(b, Sp, Hp, ndiis, conv, comm_tol=comm_tol, dp_tol=dp_tol, smin=smin,
-                                device_linalg=device_linalg))
+                                device_linalg=device_linalg, level_shift=level_shift, shift_tol=shift_tol))
     batch = GpuBatch(gbs)
     if tau_fp32 > 0.0:
         batch.set_mixed_precision(tau_fp32)
@@ -255,8 +274,14 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
         it += 1
         Ps = [st.packed_density() for st in states]
         if not incremental or Gprev is None or (it - 1) % full_every == 0:
-            batch.set_density_screening(0.0)
-            Gs = batch.rhf_form_gmatrix(Ps)
+            if tau_full > 0.0 and Gprev is not None:
+                batch.set_density_screening(tau_full)
+                Gn = batch.rhf_form_gmatrix([np.zeros_like(P) if st.converged else P
+                                             for P, st in zip(Ps, states)])
+                Gs = [Gp if st.converged else G for G, Gp, st in zip(Gn, Gprev, states)]
+            else:
+                batch.set_density_screening(0.0)
+                Gs = batch.rhf_form_gmatrix(Ps)
         else:
             dPs = [P - Pp for P, Pp in zip(Ps, Pprev)]
             big = max(float(np.abs(d).max()) for d in dPs)
