@@ -277,12 +277,13 @@ int patgpu_scf_density_host(patgpu_scf s, const double *F, double *P, double *W,
 int patgpu_set_density_screening(patgpu_handle h, double tau_dens);
 int patgpu_last_computed(patgpu_handle h, long long *quartets);
 /* Density-weighted precision of density-screened builds (no counterpart in
- * the reference): a quartet kept by the screening whose bound
- * Q_ab Q_cd max|D| is below tau32 is computed in FP32 arithmetic with FP64
- * roots, prefactors and J/K sums -- in a difference build G[P_n - P_(n-1)]
- * the density factor makes most contributions small, so their FP32 error
- * (about 1e-7 of the contribution) stays far below the screening
- * threshold's scale.  0 (the default) turns it off.  The first non-zero
+ * the reference): a quartet kept by the screening whose density-weighted
+ * term bound (the term bound of patgpu_set_mixed_precision times the same
+ * max|D|) is below tau32 is computed in FP32 arithmetic with FP64 roots,
+ * prefactors and J/K sums -- in a difference build G[P_n - P_(n-1)] the
+ * density factor makes most contributions small, so their FP32 error
+ * (about 1e-7 of the bound) stays far below the screening threshold's
+ * scale.  0 (the default) turns it off.  The first non-zero
  * value times the FP32 kernels per class. */
 int patgpu_set_density_precision(patgpu_handle h, double tau32);
 
@@ -309,9 +310,19 @@ int patgpu_batch_set_mixed_precision(patgpu_batch b, double tau_fp32);
  * second graph holding each molecule's density filter ahead of its class
  * launches (the filtered work counts stay on the device, so the graph
  * replays whatever densities the buffers hold); 0 returns to the plain
- * graph.  patgpu_batch_last_computed: quartets computed by the last launch
+ * graph.  The second graph copies both thresholds from host memory when it
+ * starts, so they may change from one launch to the next (an SCF that
+ * tightens its screening as it converges) without a new capture; change
+ * them only while no launch of the batch is pending.  The first tau32 > 0
+ * captures the graph once more with the FP32 sublist launches in it.
+ * patgpu_batch_last_computed: quartets computed by the last launch
  * (synchronises the batch's stream). */
 int patgpu_batch_set_density_screening(patgpu_batch b, double tau_dens, double tau32);
+/* The same with a threshold pair per molecule (arrays of the batch's
+ * molecule count; tau32 may be NULL for zeros), so that each molecule of an
+ * SCF can tighten its own screening as it converges.  Screening is on when
+ * any tau_dens is positive; a molecule at 0 then keeps every quartet. */
+int patgpu_batch_set_density_thresholds(patgpu_batch b, const double *tau_dens, const double *tau32);
 int patgpu_batch_last_computed(patgpu_batch b, long long *quartets);
 int patgpu_batch_launch(patgpu_batch b, void *stream);
 int patgpu_batch_rhf_gmatrix(patgpu_batch b, const double *const *P, double *const *G);
@@ -319,11 +330,15 @@ int patgpu_batch_stats(patgpu_batch b, long long *out4);
 int patgpu_batch_last_timing(patgpu_batch b, double *kernel_ns);
 
 /* Mixed precision (no counterpart in the reference, which is FP64
- * throughout): quartets whose Schwarz bound Q_ab Q_cd lies between the
- * screening threshold and tau_fp32 are computed with FP32 recursion,
- * transfer and assembly, while roots, weights, prefactors and every J/K
- * product and sum stay FP64; their integrals are below tau_fp32 in size, so
- * the absolute error per integral is about 1e-7 tau_fp32.  0 turns it off
+ * throughout): screened-in quartets whose term bound lies below tau_fp32
+ * are computed with FP32 recursion, transfer and assembly, while roots,
+ * weights, prefactors and every J/K product and sum stay FP64.  The term
+ * bound is an upper estimate of the terms the Rys scheme sums for the
+ * quartet (prefactor times, per side, (2|A-B| + share of |P-Q| +
+ * sqrt((L+1)/2p))^L), not the Schwarz bound Q_ab Q_cd: distant diffuse
+ * distributions have small integrals made of large cancelling root terms,
+ * and FP32 rounding scales with the terms.  The absolute error per
+ * integral is then about 1e-7 tau_fp32.  0 turns it off
  * (the default).  Per quartet class the library times the FP32 kernels
  * against the class's FP64 kernel on that window and keeps the fastest, so
  * a class whose window is too small to repay FP32 stays FP64 (one launch).

@@ -180,6 +180,14 @@ struct patgpu_basis {
     pg::DBuf d_soff, d_snst, d_dsh, d_flist, d_fcnt;
     std::vector<unsigned long long> fcnt;   // per class: filtered FP64, FP32 sublist counts
     bool filtered = false;                  // the current build runs over d_flist
+    // the filter reads its thresholds {tau_dens, tau_dens32} from device
+    // memory (d_scr, or a batch's copy), so that a captured graph follows
+    // threshold changes without being captured again
+    pg::DBuf d_scr;
+    // the launches of the density-weighted FP32 sublists are enqueued even
+    // while tau_dens32 is 0 (they then run no quartet): a batch sets this
+    // once its builds have used tau_dens32 > 0, so its graph stays valid
+    bool dens32_armed = false;
     long long last_computed = 0;            // quartets computed by the last host-buffer build
     // work buffers
     pg::DBuf d_D0, d_D1, d_A0, d_A1, d_Pk0, d_Pk1, d_Gk0, d_Gk1, d_err;
@@ -450,7 +458,8 @@ static EriArgs list_args(const patgpu_basis *h, const ClassWork &w, int mode, in
 static cudaError_t launch_work(const patgpu_basis *h, const ClassWork &w, const EriArgs &proto, cudaStream_t s)
 {
     const double lo = h->tau > 0.0 ? h->tau : -1.0;
-    const bool mixed = (h->tau_mix > lo && h->tau_mix > 0.0) || (h->filtered && h->tau_dens32 > 0.0);
+    const bool mixed =
+        (h->tau_mix > lo && h->tau_mix > 0.0) || (h->filtered && (h->tau_dens32 > 0.0 || h->dens32_armed));
     if (h->lists) {
         // a class whose FP32 window is kept on its FP64 kernel (tune_fp32)
         // runs both windows, adjacent in its unfiltered list, as one launch
@@ -1103,10 +1112,11 @@ __device__ __forceinline__ void warp_append(bool keep, unsigned long long v, uns
 // of mixed precision) or its density-weighted term bound (term_bound of the
 // class lab, lcd times the same density maximum) is below tau32, else to the
 // FP64 sublist (upward from out64); counts in cnt[0] and cnt[1].
-__global__ void density_filter_kernel(const EriArgs a, const double *__restrict__ dsh, int nsh, double tau,
-                                      double tau32, int all32, int lab, int lcd, unsigned long long *out64,
-                                      unsigned long long *end32, unsigned long long *cnt)
+__global__ void density_filter_kernel(const EriArgs a, const double *__restrict__ dsh, int nsh,
+                                      const double *__restrict__ scr, int all32, int lab, int lcd,
+                                      unsigned long long *out64, unsigned long long *end32, unsigned long long *cnt)
 {
+    const double tau = scr[0], tau32 = scr[1];
     for (long long qi0 = (long long)blockIdx.x * blockDim.x; qi0 < a.nquart;
          qi0 += (long long)gridDim.x * blockDim.x) {
         const long long qi = qi0 + threadIdx.x;
@@ -1128,10 +1138,11 @@ __global__ void density_filter_kernel(const EriArgs a, const double *__restrict_
 }
 
 // Filter every class's list(s) against the density of this build (d_D0, and
-// d_D1 for UHF) into d_flist, enqueued on s: the counts stay on the device
-// (the class launches read them there), so a build with the filter can be
-// captured in a CUDA graph.
-static int density_filter_enqueue(patgpu_basis *h, bool two, cudaStream_t s)
+// d_D1 for UHF) into d_flist, enqueued on s, at the thresholds scr[0] (tau)
+// and scr[1] (tau32) in device memory: the counts stay on the device (the
+// class launches read them there), so a build with the filter can be
+// captured in a CUDA graph, and its thresholds changed between replays.
+static int density_filter_enqueue(patgpu_basis *h, bool two, cudaStream_t s, const double *scr)
 {
     const int nsh = h->nsh;
     shell_dmax_kernel<<<grid_for((long long)nsh * nsh, h->num_sms), 256, 0, s>>>(
@@ -1148,7 +1159,7 @@ static int density_filter_enqueue(patgpu_basis *h, bool two, cudaStream_t s)
             if (a.nquart <= 0) continue;
             const int g = (int)std::min<long long>((a.nquart + 255) / 256, (long long)h->num_sms * 16);
             density_filter_kernel<<<std::max(g, 1), 256, 0, s>>>(
-                a, h->d_dsh.as<double>(), nsh, h->tau_dens, h->tau_dens32, win, w.la + w.lb, w.lc + w.ld, out + w.loff,
+                a, h->d_dsh.as<double>(), nsh, scr, win, w.la + w.lb, w.lc + w.ld, out + w.loff,
                 out + w.loff + w.count, h->d_fcnt.as<unsigned long long>() + 2 * w.idx);
         }
     PG_CUDA(cudaGetLastError());
@@ -1171,6 +1182,7 @@ static int density_filter_buffers(patgpu_basis *h)
     PG_CUDA(h->d_dsh.ensure(sizeof(double) * (size_t)h->nsh * h->nsh));
     PG_CUDA(h->d_flist.ensure(std::max<size_t>(h->d_list.bytes, 16)));
     PG_CUDA(h->d_fcnt.ensure(sizeof(unsigned long long) * 2 * std::max<size_t>(h->work.size(), 1)));
+    PG_CUDA(h->d_scr.ensure(2 * sizeof(double)));
     return 0;
 }
 
@@ -1208,8 +1220,10 @@ static int host_fock(patgpu_basis *h, int mode, const double *P0, const double *
     const bool filt = h->tau_dens > 0.0 && h->lists;
     if (filt) {
         if ((rc = density_filter_buffers(h))) return rc;
+        const double scr[2] = {h->tau_dens, h->tau_dens32};   // pageable: staged before the call returns
+        PG_CUDA(cudaMemcpyAsync(h->d_scr.p, scr, sizeof(scr), cudaMemcpyHostToDevice, s));
         PG_CUDA(cudaEventRecord(h->ev0, s));
-        if ((rc = density_filter_enqueue(h, mode == MODE_UHF, s))) return rc;
+        if ((rc = density_filter_enqueue(h, mode == MODE_UHF, s, h->d_scr.as<double>()))) return rc;
         h->filtered = true;
         h->fcnt.assign(2 * std::max<size_t>(h->work.size(), 1), 0);
     }
@@ -2061,7 +2075,11 @@ struct patgpu_batch_s {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int nodes[2] = {0, 0};
     int screened = 0;                      // launches use graph [1]
-    double scr_tau = 0.0, scr_tau32 = 0.0; // thresholds graph [1] was captured with
+    // the screening thresholds of graph [1], {tau_dens, tau32} per molecule:
+    // pinned host pairs that the graph's first node copies to d_scr on
+    // every replay, so new thresholds need no new capture
+    double *h_scr = nullptr;
+    pg::DBuf d_scr;
     double last_ns = 0.0;
     std::vector<double> stage;
 };
@@ -2092,9 +2110,11 @@ static int batch_enqueue(patgpu_batch_s *b, int m, cudaStream_t s, bool screened
     unpack_kernel<<<grid_for((long long)nn, h->num_sms), 256, 0, s>>>(b->dP[m].as<double>(), h->d_D0.as<double>(),
                                                                     h->n);
     if (int rc = acc_clear(h, h->d_A0.p, s)) return rc;
-    const bool filt = screened && h->tau_dens > 0.0 && h->lists;
+    // graph [1] filters every molecule with lists, at its own thresholds (a
+    // threshold of 0 keeps every quartet)
+    const bool filt = screened && h->lists;
     if (filt) {
-        if (int rc = density_filter_enqueue(h, false, s)) return rc;
+        if (int rc = density_filter_enqueue(h, false, s, b->d_scr.as<double>() + 2 * m)) return rc;
         h->filtered = true;
     }
     EriArgs a = h->base_args();
@@ -2113,6 +2133,8 @@ static int batch_capture(patgpu_batch_s *b, int k)
 {
     const bool screened = k == 1;
     const int nm = (int)b->mols.size();
+    const size_t scr_bytes = 2 * sizeof(double) * (size_t)nm;
+    if (screened) PG_CUDA(cudaMemcpyAsync(b->d_scr.p, b->h_scr, scr_bytes, cudaMemcpyHostToDevice, b->cs));
     // warm-up outside the capture: configures every kernel it will launch
     for (int m = 0; m < nm; ++m) {
         int rc = batch_enqueue(b, m, b->cs, screened);
@@ -2126,7 +2148,10 @@ static int batch_capture(patgpu_batch_s *b, int k)
                      [&](int x, int y) { return b->mols[x]->nquart > b->mols[y]->nquart; });
     PG_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
-    cudaError_t e = cudaEventRecord(b->fork, b->cs);
+    // graph [1] first copies the current thresholds from the pinned pair
+    cudaError_t e = screened ? cudaMemcpyAsync(b->d_scr.p, b->h_scr, scr_bytes, cudaMemcpyHostToDevice, b->cs)
+                             : cudaSuccess;
+    if (e == cudaSuccess) e = cudaEventRecord(b->fork, b->cs);
     for (size_t i = 0; e == cudaSuccess && i < b->side.size(); ++i) e = cudaStreamWaitEvent(b->side[i], b->fork, 0);
     for (int i = 0; e == cudaSuccess && !rc && i < nm; ++i) rc = batch_enqueue(b, order[i], b->side[i % b->side.size()], screened);
     for (size_t i = 0; e == cudaSuccess && !rc && i < b->side.size(); ++i) {
@@ -2176,6 +2201,10 @@ int patgpu_batch_create(int nmol, const patgpu_handle *mols, patgpu_batch *out)
             cudaMemset(b->dP[m].p, 0, sizeof(double) * no2) != cudaSuccess)
             return bad("device buffers");
     }
+    if (cudaMallocHost((void **)&b->h_scr, 2 * sizeof(double) * nmol) != cudaSuccess ||
+        b->d_scr.ensure(2 * sizeof(double) * nmol) != cudaSuccess)
+        return bad("threshold buffers");
+    for (int k = 0; k < 2 * nmol; ++k) b->h_scr[k] = 0.0;
     if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
@@ -2204,6 +2233,7 @@ int patgpu_batch_destroy(patgpu_batch b)
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->cs) cudaStreamDestroy(b->cs);
+    if (b->h_scr) cudaFreeHost(b->h_scr);
     delete b;
     return 0;
 }
@@ -2227,22 +2257,48 @@ int patgpu_batch_set_mixed_precision(patgpu_batch b, double tau_fp32)
     return 0;
 }
 
+int patgpu_batch_set_density_thresholds(patgpu_batch b, const double *tau_dens, const double *tau32)
+{
+    if (!b || !tau_dens) return fail(PATGPU_EINVAL, "patgpu_batch_set_density_thresholds: null argument");
+    const int nm = (int)b->mols.size();
+    bool any = false, any32 = false;
+    for (int m = 0; m < nm; ++m) {
+        const double t = tau_dens[m], t32 = tau32 ? tau32[m] : 0.0;
+        if (!(t >= 0.0) || !(t32 >= 0.0))
+            return fail(PATGPU_EINVAL, "patgpu_batch_set_density_thresholds: bad threshold of molecule %d", m);
+        any = any || t > 0.0;
+        any32 = any32 || t32 > 0.0;
+    }
+    b->screened = any ? 1 : 0;
+    if (!any) return 0;   // plain graph; graph [1] keeps its structure for later
+    // graph [1] reads the thresholds at replay: only a change of its launch
+    // structure (first use, or the first tau32 > 0) needs a new capture
+    bool recapture = !b->exec[1];
+    for (int m = 0; m < nm; ++m) {
+        patgpu_basis *h = b->mols[m];
+        const double t32 = tau32 ? tau32[m] : 0.0;
+        if (any32 && !h->dens32_armed) {
+            int rc = patgpu_set_density_precision(h, std::max(t32, 1e-300));
+            if (rc) return rc;
+            h->dens32_armed = true;
+            recapture = true;
+        }
+        h->tau_dens = tau_dens[m];
+        h->tau_dens32 = t32;
+        if (h->lists)
+            if (int rc = density_filter_buffers(h)) return rc;
+        b->h_scr[2 * m] = tau_dens[m];
+        b->h_scr[2 * m + 1] = t32;
+    }
+    if (recapture) batch_drop_graph(b, 1);
+    return 0;
+}
+
 int patgpu_batch_set_density_screening(patgpu_batch b, double tau_dens, double tau32)
 {
     if (!b || !(tau_dens >= 0.0) || !(tau32 >= 0.0)) return fail(PATGPU_EINVAL, "bad batch screening threshold");
-    b->screened = tau_dens > 0.0 ? 1 : 0;
-    if (!b->screened) return 0;   // plain graph; the handles' screening stays for graph [1]
-    if (b->exec[1] && tau_dens == b->scr_tau && tau32 == b->scr_tau32) return 0;
-    for (auto *h : b->mols) {
-        int rc = patgpu_set_density_screening(h, tau_dens);
-        if (!rc) rc = patgpu_set_density_precision(h, tau_dens > 0.0 ? tau32 : 0.0);
-        if (!rc && tau_dens > 0.0 && h->lists) rc = density_filter_buffers(h);
-        if (rc) return rc;
-    }
-    b->scr_tau = tau_dens;
-    b->scr_tau32 = tau32;
-    batch_drop_graph(b, 1);
-    return 0;
+    const std::vector<double> t(b->mols.size(), tau_dens), t32(b->mols.size(), tau32);
+    return patgpu_batch_set_density_thresholds(b, t.data(), t32.data());
 }
 
 int patgpu_batch_last_computed(patgpu_batch b, long long *quartets)
@@ -2251,7 +2307,7 @@ int patgpu_batch_last_computed(patgpu_batch b, long long *quartets)
     long long tot = 0;
     PG_CUDA(cudaStreamSynchronize(b->cs));
     for (auto *h : b->mols) {
-        if (!b->screened || !(h->tau_dens > 0.0) || !h->lists) {
+        if (!b->screened || !h->lists) {
             tot += h->nquart;
             continue;
         }

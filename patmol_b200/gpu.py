@@ -83,6 +83,7 @@ def lib():
         L.patgpu_set_density_screening.argtypes = [H, ctypes.c_double]
         L.patgpu_set_density_precision.argtypes = [H, ctypes.c_double]
         L.patgpu_batch_set_density_screening.argtypes = [H, ctypes.c_double, ctypes.c_double]
+        L.patgpu_batch_set_density_thresholds.argtypes = [H, dp, dp]
         L.patgpu_batch_last_computed.argtypes = [H, lp]
         L.patgpu_last_computed.argtypes = [H, lp]
         L.patgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(H), ctypes.POINTER(H)]
@@ -287,8 +288,8 @@ class GpuBasis:
         _check(lib().patgpu_set_density_precision(self.h, float(tau32)), "set_density_precision")
 
     def set_mixed_precision(self, tau_fp32: float) -> int:
-        """FP32 arithmetic for quartets with Schwarz bound below tau_fp32
-        (FP64 accumulation); returns how many quartets run in FP32."""
+        """FP32 arithmetic for quartets whose Rys-term bound is below
+        tau_fp32 (FP64 accumulation); returns how many quartets run in FP32."""
         _check(lib().patgpu_set_mixed_precision(self.h, float(tau_fp32)), "set_mixed_precision")
         n = ctypes.c_longlong()
         _check(lib().patgpu_mixed_stats(self.h, ctypes.byref(n)), "mixed_stats")
@@ -342,6 +343,16 @@ class GpuBatch:
         molecule's build: launches then replay the screened graph."""
         _check(lib().patgpu_batch_set_density_screening(self.b, float(tau_dens), float(tau32)),
                "batch_set_density_screening")
+
+    def set_density_thresholds(self, tau_dens, tau32=None):
+        """Per-molecule density screening thresholds (and density-weighted
+        FP32 thresholds); the screened graph reads them at every launch."""
+        t = np.ascontiguousarray(tau_dens, dtype=np.float64)
+        t32 = np.zeros_like(t) if tau32 is None else np.ascontiguousarray(tau32, dtype=np.float64)
+        if t.shape != (len(self.mols),) or t32.shape != t.shape:
+            raise ValueError("one threshold per molecule")
+        _check(lib().patgpu_batch_set_density_thresholds(self.b, _p(t, ctypes.c_double), _p(t32, ctypes.c_double)),
+               "batch_set_density_thresholds")
 
     def last_computed(self) -> int:
         n = ctypes.c_longlong()

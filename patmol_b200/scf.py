@@ -209,7 +209,7 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
     from a full build.  device_linalg=True diagonalises on the GPU.
-    tau_fp32 > 0 runs quartets whose Schwarz bound is below it in FP32
+    tau_fp32 > 0 runs quartets whose Rys-term bound is below it in FP32
     (mixed precision) in every build.  level_shift > 0 raises the virtual
     orbitals by that many Eh while the DIIS error exceeds shift_tol."""
     gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
@@ -240,11 +240,11 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
               tau_inc32: float = 0.0, fp32_dp_min: float = 1e-4, full_every: int = 8, comm_tol: float = 1e-9,
               dp_tol: float = 1e-8, computed: list | None = None, smin: float = 1e-10,
               device_linalg: bool = False, fock_seconds: list | None = None, level_shift: float = 0.0,
-              shift_tol: float = 1e-3, tau_full: float = 0.0):
+              shift_tol: float = 1e-3, tau_full: float = 0.0, tau_rel: float = 0.0, tau_max: float = 1e-8):
     """Closed-shell SCF of many molecules in lock step: every iteration is one
     batched Fock build (one CUDA graph over all molecules, patgpu_batch_*),
     then each molecule's host step.  Converged molecules keep their density.
-    tau_fp32 > 0 runs quartets with Schwarz bound below it in FP32.
+    tau_fp32 > 0 runs quartets with Rys-term bound below it in FP32.
     incremental=True: between full builds (the first and every full_every-th
     iteration) the graph builds G[P_n - P_(n-1)] of every molecule with
     density screening at tau_inc (the filter runs inside the graph) and adds
@@ -256,9 +256,16 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
     full builds of the iterations by the density as well, at that bound, and
     gives converged molecules a zero density there, so that they cost
     nothing after convergence.  The final energies come from an unscreened
-    full build.  level_shift / shift_tol as in rhf().  computed, if given,
-    receives the quartets of every build, and fock_seconds the device-timed
-    seconds of every batched build."""
+    full build.  tau_rel > 0 tightens the screening with the SCF: each
+    molecule's build is screened at tau_rel times its own DIIS error,
+    clipped to [tau_inc, tau_max] (the first build at tau_max): early
+    iterations, whose Fock matrices are far from self-consistent anyway,
+    drop many more quartets, and the error each build's screening adds stays
+    far below the error the molecule's SCF has left; the full builds of the
+    iterations use the same thresholds.  level_shift /
+    shift_tol as in rhf().  computed, if given, receives the quartets of
+    every build, and fock_seconds the device-timed seconds of every batched
+    build."""
     gbs = [GpuBasis(b, schwarz_tau=schwarz_tau) for b in bases]
     states = []
     for b, gb in zip(bases, gbs):
@@ -270,12 +277,25 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
         batch.set_mixed_precision(tau_fp32)
     it = 0
     Gprev = Pprev = None
+
+    def thresholds(floor):
+        # per molecule: adaptive (tau_rel > 0: its own DIIS error) or fixed
+        out = []
+        for st in states:
+            e = st.err
+            out.append(floor if tau_rel <= 0.0 else
+                       (tau_max if not np.isfinite(e) else min(tau_max, max(floor, tau_rel * e))))
+        return out
+
     while it < maxit and not all(st.converged for st in states):
         it += 1
         Ps = [st.packed_density() for st in states]
         if not incremental or Gprev is None or (it - 1) % full_every == 0:
-            if tau_full > 0.0 and Gprev is not None:
-                batch.set_density_screening(tau_full)
+            if tau_rel > 0.0 and Gprev is None:
+                batch.set_density_screening(tau_max)
+                Gs = batch.rhf_form_gmatrix(Ps)
+            elif (tau_full > 0.0 or tau_rel > 0.0) and Gprev is not None:
+                batch.set_density_thresholds(thresholds(max(tau_full, 1e-14)))
                 Gn = batch.rhf_form_gmatrix([np.zeros_like(P) if st.converged else P
                                              for P, st in zip(Ps, states)])
                 Gs = [Gp if st.converged else G for G, Gp, st in zip(Gn, Gprev, states)]
@@ -284,8 +304,8 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
                 Gs = batch.rhf_form_gmatrix(Ps)
         else:
             dPs = [P - Pp for P, Pp in zip(Ps, Pprev)]
-            big = max(float(np.abs(d).max()) for d in dPs)
-            batch.set_density_screening(tau_inc, tau_inc32 if big > fp32_dp_min else 0.0)
+            t32 = [tau_inc32 if float(np.abs(d).max()) > fp32_dp_min else 0.0 for d in dPs]
+            batch.set_density_thresholds(thresholds(tau_inc), t32)
             Gs = [Gp + dG for Gp, dG in zip(Gprev, batch.rhf_form_gmatrix(dPs))]
         if computed is not None:
             computed.append(batch.last_computed())

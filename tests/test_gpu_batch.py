@@ -4,7 +4,7 @@ molecules of uneven size.
   * every molecule's G from the batch equals its own handle's G within
     1e-11 (the same kernels; only the order of FP64 atomic adds differs),
     on the first (captured) and a replayed launch;
-  * the mixed-precision batch (Schwarz bound < 1e-8 in FP32) stays within
+  * the mixed-precision batch (Rys-term bound < 1e-8 in FP32) stays within
     1e-6 Eh of the FP64 batch in every molecule's SCF energy;
   * the lock-step SCF reproduces each molecule's own SCF energy to 1e-9 Eh.
 """
@@ -64,20 +64,48 @@ def test_batch_mixed_precision_energy():
         assert abs(a.energy - b.energy) < 1e-6, (a.energy, b.energy)
 
 
-def test_batch_incremental_scf_matches_plain_scf():
+@pytest.mark.parametrize("tau_rel", [0.0, 1e-7])
+def test_batch_incremental_scf_matches_plain_scf(tau_rel):
     """Lock-step SCF with density-screened difference builds inside the batch
-    graph (density-weighted FP32 while the density moves) and the
-    Schwarz-window FP32 of full builds: every molecule's energy within 1e-6
-    Eh of its own plain FP64 SCF, and the difference builds compute fewer
-    quartets than the full ones."""
+    graph (density-weighted FP32 while the density moves) and the FP32
+    window of full builds, with fixed screening and with each molecule's
+    threshold following its own DIIS error (tau_rel): every molecule's
+    energy within 1e-6 Eh of its own plain FP64 SCF, and the difference
+    builds compute fewer quartets than the full ones."""
     bases = molecules([3, 5, 4, 6], seed0=700)
     kw = dict(maxit=150, conv=1e-10, comm_tol=1e-6, dp_tol=1e-6)
     plain = [scf.rhf(b, **kw) for b in bases]
     computed = []
     inc = scf.rhf_batch(bases, tau_fp32=1e-8, incremental=True, tau_inc=1e-11, tau_inc32=1e-5,
-                        computed=computed, **kw)
+                        computed=computed, tau_rel=tau_rel, **kw)
     assert all(r.converged for r in plain) and all(r.converged for r in inc)
     for a, b in zip(plain, inc):
         assert abs(a.energy - b.energy) < 1e-6, (a.energy, b.energy)
     full = computed[0]
     assert len(computed) > 2 and min(computed[1:]) < full, computed
+
+
+def test_batch_per_molecule_thresholds_replayed():
+    """patgpu_batch_set_density_thresholds: each molecule's filter reads its
+    own threshold pair, and the screened graph reads them at every launch
+    (no new capture).  A threshold far below every bound keeps all of a
+    molecule's quartets (its own unscreened G); one far above every bound
+    keeps none (G = 0); swapping the two swaps the results."""
+    bases = molecules([3, 4, 2], seed0=900)
+    gbs = [gpu.GpuBasis(b) for b in bases]
+    batch = gpu.GpuBatch(gbs)
+    Ps = [seeded_density(b.norb, 60 + i) for i, b in enumerate(bases)]
+    ref = [g.rhf_form_gmatrix(P) for g, P in zip(gbs, Ps)]
+    for taus in ([1e-300, 1e30, 1e-300], [1e30, 1e-300, 1e30]):
+        batch.set_density_thresholds(taus)
+        nodes = batch.stats()["graph_nodes"]
+        Gs = batch.rhf_form_gmatrix(Ps)
+        for G, R, t in zip(Gs, ref, taus):
+            if t < 1.0:
+                assert np.abs(G - R).max() < 1e-11
+            else:
+                assert np.abs(G).max() == 0.0
+        kept = sum(g.stats()["quartets"] for g, t in zip(gbs, taus) if t < 1.0)
+        assert batch.last_computed() == kept
+    assert batch.stats()["graph_nodes"] == nodes
+    batch.close()

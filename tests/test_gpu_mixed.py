@@ -1,7 +1,8 @@
-"""Mixed precision: quartets whose Schwarz bound is below 1e-8 run in FP32
+"""Mixed precision: quartets whose Rys-term bound is below 1e-8 run in FP32
 arithmetic with FP64 accumulation.  Checked against the all-FP64 build at a
 physical density (the core-Hamiltonian guess): the first-order energy error
-tr(P dG) must stay below 1e-6 Eh and G below 1e-7 elementwise."""
+tr(P dG) must stay below 1e-6 Eh and G below 1e-9 elementwise (the
+term bound keeps each FP32 integral's error near 1e-7 of 1e-8)."""
 import numpy as np
 import pytest
 
@@ -48,7 +49,7 @@ def test_mixed_water_spdf_positron(variant32, monkeypatch):
         monkeypatch.setenv("PATGPU_VARIANT32", variant32)
     nfp32, nq, dg, de = mixed_vs_fp64(configs.water_spdf_positron())
     assert nfp32 > 0 if variant32 else 0 <= nfp32 < nq
-    assert dg < 1e-7 and abs(de) < 1e-6, (nfp32, nq, dg, de)
+    assert dg < 1e-9 and abs(de) < 1e-6, (nfp32, nq, dg, de)
 
 
 def test_mixed_organic_molecule():
@@ -57,14 +58,14 @@ def test_mixed_organic_molecule():
     b = configs.organic_basis(8, seed=3)
     nfp32, nq, dg, de = mixed_vs_fp64(b)
     assert nfp32 > 0
-    assert dg < 1e-7 and abs(de) < 1e-6, (nfp32, nq, dg, de)
+    assert dg < 1e-9 and abs(de) < 1e-6, (nfp32, nq, dg, de)
 
 
-@pytest.mark.parametrize("variant32", ["smem", "lane"])
+@pytest.mark.parametrize("variant32", ["smem", "lane", "warp"])
 def test_mixed_each_fp32_kernel(variant32, monkeypatch):
-    """Both FP32 kernels (shared-memory and lane), forced for every class."""
+    """Each FP32 kernel (shared-memory, lane, warp), forced for every class."""
     monkeypatch.setenv("PATGPU_VARIANT32", variant32)
     b = configs.organic_basis(6, seed=4)
     nfp32, nq, dg, de = mixed_vs_fp64(b)
-    assert nfp32 > 0.05 * nq
-    assert dg < 1e-7 and abs(de) < 1e-6, (variant32, nfp32, nq, dg, de)
+    assert nfp32 > 0.01 * nq
+    assert dg < 1e-9 and abs(de) < 1e-6, (variant32, nfp32, nq, dg, de)
