@@ -69,6 +69,8 @@ def parse():
                     help="SCF-iteration leg: screening of the mixed batch's builds at this times the largest DIIS "
                          "error, clipped to [--scf-tau-inc, --scf-tau-max] (0: fixed --scf-tau-inc)")
     ap.add_argument("--scf-tau-max", type=float, default=1e-8)
+    ap.add_argument("--scf-ediis", type=int, default=1,
+                    help="SCF-iteration leg: 1 blends energy-DIIS into DIIS while the DIIS error is above 1e-4")
     ap.add_argument("--scf-molecules", type=int, default=8,
                     help="molecules of the SCF-iteration leg (config-3 recipe); 0 skips it")
     ap.add_argument("--scf-max-atoms", type=int, default=24,
@@ -286,8 +288,9 @@ def scf_iteration_leg(a, torch):
              screening threshold follows the SCF: tau_rel times the largest
              DIIS error still iterating, clipped to [tau_inc, tau_max]; the
              final energies come from unscreened builds.
-    Both use DIIS, a 0.3 Eh virtual level shift while the DIIS error is
-    above 1e-3, the device eigensolver and canonical orthogonalisation over
+    Both use DIIS with energy-DIIS blended in while the DIIS error is above
+    1e-4, a 0.3 Eh virtual level shift while it is above 1e-3, the device
+    eigensolver and canonical orthogonalisation over
     overlap eigenvalues above 1e-7 (the diffuse 0.08 s exponents on atoms
     2.6-2.9 bohr apart make the overlap nearly singular), converged at
     |dE| < 1e-8 Eh, max|FPS-SPF| < 1e-5, max|dP| < 1e-5, at most scf_maxit
@@ -304,7 +307,7 @@ def scf_iteration_leg(a, torch):
     sizes = rng.integers(3, a.scf_max_atoms + 1, size=a.scf_molecules)
     bases = [configs.organic_basis(int(k), 3000 + i, with_f=False) for i, k in enumerate(sizes)]
     kw = dict(conv=1e-8, comm_tol=1e-5, dp_tol=1e-5, maxit=a.scf_maxit, smin=1e-7, device_linalg=True,
-              level_shift=a.scf_level_shift, shift_tol=1e-3)
+              level_shift=a.scf_level_shift, shift_tol=1e-3, ediis=bool(a.scf_ediis))
     mix = dict(tau_fp32=a.tau_fp32, incremental=True, tau_inc=a.scf_tau_inc, tau_inc32=1e-6,
                full_every=a.scf_full_every, tau_full=a.scf_tau_full, tau_rel=a.scf_tau_rel, tau_max=a.scf_tau_max)
     torch.cuda.synchronize()

@@ -62,6 +62,9 @@ struct WarpShape {
     // staged density blocks per set: D(ab), D(bd), D(bc), D(ad), D(ac)
     static constexpr int OBD = NAB, OBC = OBD + NB * ND, OAD = OBC + NB * NC, OAC = OAD + NA * ND;
     static constexpr int NDB = OAC + NA * NC;
+    // staged density words per set: only D(ab) when the exchange densities
+    // live in registers (DREG), all five blocks otherwise
+    static constexpr int NDBS = DREG ? NAB : NDB;
     static constexpr int PS = 2 * NA + 2 * NB;              // exchange partials per lane and set
     // Shared-memory strides, chosen against bank conflicts.  Each lane's
     // recursion job writes one table of TSZ entries and each lane stores its
@@ -79,8 +82,14 @@ struct WarpShape {
     static constexpr int TABD = (3 * NR * TST * (int)sizeof(R) + 7) / 8;
     static constexpr int PART = NL > 1 ? NL * PSP * NDEN : 0;
     static constexpr int REGION = TABD > PART ? TABD : PART;
-    static constexpr int WCH = NL > 1 ? CH * NL : 0;
-    static constexpr int TEAM0 = RW + NDB * NDEN + REGION + WCH;
+    // one chunk's J(ab) partials [CH][NL]; with a single bra chunk the tables
+    // are dead once it is assembled, so the partials reuse their region
+    // (WALIAS) and the team's shared memory shrinks by CH*NL words -- with
+    // NDBS, enough to fit a fourth block on an SM for the (dp|xs), (dp|ds),
+    // (pp|ss) and (dp|fs)-type classes
+    static constexpr bool WALIAS = NL > 1 && NCH == 1 && CH * NL <= REGION;
+    static constexpr int WCH = (NL > 1 && !WALIAS) ? CH * NL : 0;
+    static constexpr int TEAM0 = RW + NDBS * NDEN + REGION + WCH;
     static constexpr int TEAM = sizeof(R) == 8 ? TEAM0 + (((NL * TST - TEAM0) % 16) + 16) % 16 : TEAM0;
     // teams per warp: 32/NL, fewer where the teams' shared memory would pass
     // 28 KB a warp (the large-bra classes with one or three ket lanes), so
@@ -101,7 +110,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
     using S = WarpShape<LA, LB, LC, LD, NDEN, R>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NAB = S::NAB;
     constexpr int NR = S::NR, TAB = S::TAB, TST = S::TST, NL = S::NL, Q = S::Q;
-    constexpr int NCH = S::NCH, CH = S::CH, NDB = S::NDB, PSP = S::PSP;
+    constexpr int NCH = S::NCH, CH = S::CH, NDB = S::NDB, NDBS = S::NDBS, PSP = S::PSP;
     extern __shared__ double smem[];
 
     const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
@@ -109,9 +118,9 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
     const bool in_team = team < Q;
     double *s_rw = smem + (size_t)(warp * Q + (in_team ? team : 0)) * S::TEAM;
     double *s_db = s_rw + S::RW;
-    double *s_tab = s_db + NDB * NDEN;          // tables; after the assembly, the exchange partials
+    double *s_tab = s_db + NDBS * NDEN;         // tables; after the assembly, the exchange partials
     double *s_part = s_tab;
-    double *s_wc = s_tab + S::REGION;           // one chunk's J(ab) partials [CH][NL]
+    double *s_wc = S::WALIAS ? s_tab : s_tab + S::REGION;   // one chunk's J(ab) partials [CH][NL]
 
     const int ic = lt / ND, id = lt - (lt / ND) * ND;
     const int ecx = c_cart[LC][ic], edx = c_cart[LD][id];
@@ -172,7 +181,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
 #pragma unroll
             for (int s = 0; s < NDEN; ++s) {
                 const double *D = s == 0 ? args.D0 : args.D1;
-                double *db = s_db + s * NDB;
+                double *db = s_db + s * NDBS;
                 for (int t = lt; t < NAB; t += NL) {
                     const int ir = t / NB, icn = t - (t / NB) * NB;
                     db[t] = __ldg(D + (size_t)(fa + ir) * n + fb + icn) * c_norm[LA][ir] * c_norm[LB][icn];
@@ -275,15 +284,18 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
             R acc[CH];
 #pragma unroll
             for (int j = 0; j < CH; ++j) acc[j] = R(0);
+            if (work) assemble<LA, LB, NR, TST, c * CH, CH>(acc, X, Y, Z);
+            // the J(ab) partials below overwrite the tables (WALIAS): every
+            // lane of the warp has finished its table reads first
+            if constexpr (S::WALIAS) __syncwarp();
             if (work) {
-                assemble<LA, LB, NR, TST, c * CH, CH>(acc, X, Y, Z);
 #pragma unroll
                 for (int j = 0; j < CHN; ++j) {
                     const int ab = c * CH + j;
                     const int ia = ab / NB, ib = ab % NB;
                     const double I = (double)acc[j];
                     double dab = s_db[ab];
-                    if (NDEN == 2) dab += s_db[NDB + ab];
+                    if (NDEN == 2) dab += s_db[NDBS + ab];
                     jcd = fma(I, dab, jcd);
                     if constexpr (NL > 1) {
                         s_wc[j * NL + lt] = I * Dcd;
@@ -301,7 +313,7 @@ __global__ void __launch_bounds__(128, 4) eri_warp_kernel(const EriArgs args)
                             Pbc[s][ib] = fma(I, dad[s][ia], Pbc[s][ib]);
                             Pbd[s][ib] = fma(I, dac[s][ia], Pbd[s][ib]);
                         } else {
-                            const double *db = s_db + s * NDB;
+                            const double *db = s_db + s * NDBS;
                             Pac[s][ia] = fma(I, db[S::OBD + ib * ND + id], Pac[s][ia]);
                             Pad[s][ia] = fma(I, db[S::OBC + ib * NC + ic], Pad[s][ia]);
                             Pbc[s][ib] = fma(I, db[S::OAD + ia * ND + id], Pbc[s][ib]);

@@ -62,7 +62,7 @@ class _RHFState:
 
     def __init__(self, basis: Basis, Sp, Hp, ndiis: int, conv: float, device_linalg: bool = False,
                  comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10, level_shift: float = 0.0,
-                 shift_tol: float = 1e-3):
+                 shift_tol: float = 1e-3, ediis: bool = False):
         if basis.nelec % 2 or basis.mult != 1:
             raise ValueError("closed-shell SCF needs an even electron count and multiplicity 1")
         self.n = basis.norb
@@ -75,6 +75,11 @@ class _RHFState:
         # virtual-orbital level shift while the DIIS error is above shift_tol
         self.level_shift, self.shift_tol = level_shift, shift_tol
         self.err = np.inf
+        # EDIIS (energy-DIIS) while the DIIS error is large: densities and
+        # energies of the stored Fock matrices, and M[i, j] = tr(P_i F_j)
+        self.ediis = ediis
+        self.ps, self.ens = [], []
+        self.M = np.zeros((0, 0))
         # the step of rhf_scf_update after F (X^T F X, diagonalise, C, P) on the
         # GPU (patgpu_scf_*) or on the host
         self.linalg = GpuScfLinalg(self.X, self.nocc) if device_linalg else None
@@ -108,7 +113,10 @@ class _RHFState:
         err = F @ self.P @ self.S - self.S @ self.P @ F
         self.fs.append(F)
         self.es.append(self.X.T @ err @ self.X)
+        if self.ediis:
+            self._ediis_push(self.P, F, energy)
         self.fs, self.es = self.fs[-self.ndiis:], self.es[-self.ndiis:]
+        F_last = F
         if len(self.fs) > 1:
             m = len(self.fs)
             B = -np.ones((m + 1, m + 1))
@@ -124,6 +132,12 @@ class _RHFState:
             except np.linalg.LinAlgError:
                 pass
         self.err = float(np.max(np.abs(self.es[-1])))
+        if self.ediis and len(self.fs) > 1 and self.err > 1e-4:
+            # energy-DIIS far from convergence, blended into DIIS between
+            # DIIS errors 1e-1 and 1e-4 (weight 10 x error)
+            Fe = self._ediis_fock(F_last)
+            w = min(1.0, 10.0 * self.err)
+            F = w * Fe + (1.0 - w) * F
         if self.level_shift > 0.0 and self.err > self.shift_tol:
             # F + s (S - S P S) raises the virtual space of the current
             # orbitals by s (P S P = P): damps occupied-virtual rotations and
@@ -138,6 +152,50 @@ class _RHFState:
                 self.err < self.comm_tol and dP < self.dp_tol:
             self.converged = True
         self.e_old = energy
+
+    def _ediis_push(self, P, F, energy):
+        self.ps.append(P)
+        self.ens.append(energy)
+        fs = self.fs[-len(self.ps):]
+        m = len(self.ps)
+        M = np.zeros((m, m))
+        M[:m - 1, :m - 1] = self.M
+        for j in range(m):
+            M[m - 1, j] = np.sum(P * fs[j])
+            M[j, m - 1] = np.sum(self.ps[j] * F)
+        k = max(0, m - self.ndiis)
+        self.ps, self.ens, self.M = self.ps[k:], self.ens[k:], M[k:, k:]
+
+    def _ediis_fock(self, F_fallback):
+        """sum_i c_i F_i with c on the simplex minimising the energy of the
+        interpolated density, E(c) = sum c_i E_i - 1/2 sum c_i c_j
+        tr((P_i - P_j)(F_i - F_j)) -- exact for the closed-shell energy,
+        which is quadratic in P (Kudin, Scuseria and Cances, J. Chem. Phys.
+        116, 8255 (2002)); c = t^2 / |t|^2 keeps c on the simplex."""
+        from scipy.optimize import minimize
+        E = np.array(self.ens)
+        M = self.M
+        d = np.diag(M)
+        D = d[:, None] + d[None, :] - M - M.T
+        m = len(E)
+        fs = self.fs[-m:]
+
+        def f(t):
+            t2 = t * t
+            s = t2.sum()
+            c = t2 / s
+            val = c @ E - 0.5 * c @ D @ c
+            gc = E - D @ c
+            return val, 2.0 * t * (gc - c @ gc) / s
+
+        t0 = np.ones(m) / np.sqrt(m)
+        t0[-1] *= 2.0
+        try:
+            r = minimize(f, t0, jac=True, method="BFGS", options={"maxiter": 200})
+            c = r.x * r.x / np.sum(r.x * r.x)
+        except Exception:
+            return F_fallback
+        return sum(ci * Fi for ci, Fi in zip(c, fs))
 
     def finish(self, Gp) -> RHFResult:
         """Energy and orbitals of the final density."""
@@ -205,19 +263,21 @@ def rhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
         maxit: int = 100, schwarz_tau: float = 1e-14, ndiis: int = 8, incremental: bool = False,
         tau_inc: float = 1e-14, device_linalg: bool = False, tau_fp32: float = 0.0, tau_inc32: float = 0.0,
         comm_tol: float = 1e-9, dp_tol: float = 1e-8, smin: float = 1e-10, level_shift: float = 0.0,
-        shift_tol: float = 1e-3, full_every: int = 8) -> RHFResult:
+        shift_tol: float = 1e-3, full_every: int = 8, ediis: bool = False) -> RHFResult:
     """Closed-shell SCF.  incremental=True builds G from density differences
     (IncrementalFock) during the iterations; the final energy always comes
     from a full build.  device_linalg=True diagonalises on the GPU.
     tau_fp32 > 0 runs quartets whose Rys-term bound is below it in FP32
     (mixed precision) in every build.  level_shift > 0 raises the virtual
-    orbitals by that many Eh while the DIIS error exceeds shift_tol."""
+    orbitals by that many Eh while the DIIS error exceeds shift_tol.
+    ediis=True blends energy-DIIS into DIIS while the DIIS error is above
+    1e-4 (_RHFState._ediis_fock)."""
     gb = gpu if gpu is not None else GpuBasis(basis, schwarz_tau=schwarz_tau)
     Sp, Hp = _setup(gb, dpm)
     if tau_fp32 > 0.0:
         gb.set_mixed_precision(tau_fp32)
     st = _RHFState(basis, Sp, Hp, ndiis, conv, device_linalg=device_linalg, comm_tol=comm_tol, dp_tol=dp_tol,
-                   smin=smin, level_shift=level_shift, shift_tol=shift_tol)
+                   smin=smin, level_shift=level_shift, shift_tol=shift_tol, ediis=ediis)
     fock = IncrementalFock(gb, tau_inc, full_every=full_every, tau32=tau_inc32) if incremental else None
     fock_ns = 0.0
     while st.it < maxit and not st.converged:
@@ -240,7 +300,8 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
               tau_inc32: float = 0.0, fp32_dp_min: float = 1e-4, full_every: int = 8, comm_tol: float = 1e-9,
               dp_tol: float = 1e-8, computed: list | None = None, smin: float = 1e-10,
               device_linalg: bool = False, fock_seconds: list | None = None, level_shift: float = 0.0,
-              shift_tol: float = 1e-3, tau_full: float = 0.0, tau_rel: float = 0.0, tau_max: float = 1e-8):
+              shift_tol: float = 1e-3, tau_full: float = 0.0, tau_rel: float = 0.0, tau_max: float = 1e-8,
+              ediis: bool = False):
     """Closed-shell SCF of many molecules in lock step: every iteration is one
     batched Fock build (one CUDA graph over all molecules, patgpu_batch_*),
     then each molecule's host step.  Converged molecules keep their density.
@@ -263,7 +324,7 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
     drop many more quartets, and the error each build's screening adds stays
     far below the error the molecule's SCF has left; the full builds of the
     iterations use the same thresholds.  level_shift /
-    shift_tol as in rhf().  computed, if given, receives the quartets of
+    shift_tol / ediis as in rhf().  computed, if given, receives the quartets of
     every build, and fock_seconds the device-timed seconds of every batched
     build."""
     gbs = [GpuBasis(b, schwarz_tau=schwarz_tau) for b in bases]
@@ -271,7 +332,8 @@ def rhf_batch(bases, dpm: bool = False, tau_fp32: float = 0.0, conv: float = 1e-
     for b, gb in zip(bases, gbs):
         Sp, Hp = _setup(gb, dpm)
         states.append(_RHFState(b, Sp, Hp, ndiis, conv, comm_tol=comm_tol, dp_tol=dp_tol, smin=smin,
-                                device_linalg=device_linalg, level_shift=level_shift, shift_tol=shift_tol))
+                                device_linalg=device_linalg, level_shift=level_shift, shift_tol=shift_tol,
+                                ediis=ediis))
     batch = GpuBatch(gbs)
     if tau_fp32 > 0.0:
         batch.set_mixed_precision(tau_fp32)
