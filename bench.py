@@ -36,15 +36,15 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "water s/p/d/f + ghost positron s/p/d shells (87 shells, 292 functions), RHF Fock build"
 
-# DRAM bytes (read + write) of the 55 class kernels of one Fock build of this
-# workload, from one ncu capture of dram__bytes_read.sum and
-# dram__bytes_write.sum (cold caches per launch); the capture's command and
+# DRAM bytes (read + write) of the 55 class kernels and the unpack/finish
+# kernels of one Fock build of this workload, from one ncu capture of
+# dram__bytes_read.sum and dram__bytes_write.sum (cold caches per launch,
+# the tuner's choices of a normal run replayed); the capture's command and
 # per-kernel figures are kept with the other ncu summaries under profiles/.
-STEP_DRAM_BYTES = 194.7e6
-STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 55 class kernels of one "
-                    "Fock build (91.6 MB read incl. 58 MB of compacted quartet lists, 103.1 MB write, mostly "
-                    "local-memory write-back of f-heavy lane-kernel classes); captured before the "
-                    "occupancy-hinted shared-memory variant, which four f classes now use")
+STEP_DRAM_BYTES = 114.6e6
+STEP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum over the 57 launches of one Fock build "
+                    "(103.1 MB read, 58 MB of it the compacted quartet lists; 11.5 MB written, lane-kernel "
+                    "spills of d/f classes), tuner choices replayed with PATGPU_TUNE_LOAD")
 
 
 def parse():

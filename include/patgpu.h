@@ -295,7 +295,9 @@ int patgpu_set_density_precision(patgpu_handle h, double tau32);
  * computes dG_m = G[dP_m] (RHF, overwritten) for every molecule as ONE
  * CUDA graph launch on `stream`; the graph is captured on the first launch
  * (after one plain build per molecule) and holds each molecule's class
- * launches, spread over parallel capture streams.  patgpu_batch_rhf_gmatrix
+ * launches, spread over parallel capture streams or kept on one: the first
+ * capture of each graph kind (plain, density-screened) times both forms once
+ * on the buffers' densities and keeps the faster.  patgpu_batch_rhf_gmatrix
  * is the host-buffer form (G_m += G[P_m]).  Mixed precision is per
  * molecule; patgpu_batch_set_mixed_precision sets it for all and drops the
  * graph.  Stats: [0] molecules, [1] quartets, [2] FP32 quartets, [3]

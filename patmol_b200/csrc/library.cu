@@ -2057,8 +2057,9 @@ int patgpu_dpm(patgpu_handle h, double *H)
 // ================================================================ batches
 // Many molecules advanced together: one CUDA graph holds every molecule's
 // Fock build (density unpack, accumulator clear, its quartet-class launches
-// in class order, the symmetrising finish), spread over kBatchStreams
-// capture streams so the small per-molecule grids run side by side.  The
+// in class order, the symmetrising finish), spread over up to kBatchStreams
+// capture streams so that molecules can run side by side, or kept on one
+// (batch_capture times both on the first capture of each graph kind).  The
 // graph is captured on the first launch (after one plain warm-up build per
 // molecule, which also configures every kernel) and replayed afterwards;
 // changing a molecule's mixed-precision threshold drops it.
@@ -2074,6 +2075,8 @@ struct patgpu_batch_s {
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int nodes[2] = {0, 0};
+    // side streams each graph spreads the molecules over (0: not chosen yet)
+    int nside[2] = {0, 0};
     int screened = 0;                      // launches use graph [1]
     // the screening thresholds of graph [1], {tau_dens, tau32} per molecule:
     // pinned host pairs that the graph's first node copies to d_scr on
@@ -2129,6 +2132,52 @@ static int batch_enqueue(patgpu_batch_s *b, int m, cudaStream_t s, bool screened
     return finish(h, h->d_A0.as<double>(), b->dG[m].as<double>(), s);
 }
 
+// Capture graph [k] over ns of the side streams into *g / *x.
+static int batch_capture_streams(patgpu_batch_s *b, int k, int ns, cudaGraph_t *g, cudaGraphExec_t *x)
+{
+    const bool screened = k == 1;
+    const int nm = (int)b->mols.size();
+    const size_t scr_bytes = 2 * sizeof(double) * (size_t)nm;
+    // heaviest molecules first, dealt round-robin over the capture streams
+    std::vector<int> order(nm);
+    for (int m = 0; m < nm; ++m) order[m] = m;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return b->mols[x]->nquart > b->mols[y]->nquart; });
+    PG_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    // graph [1] first copies the current thresholds from the pinned pairs
+    cudaError_t e = screened ? cudaMemcpyAsync(b->d_scr.p, b->h_scr, scr_bytes, cudaMemcpyHostToDevice, b->cs)
+                             : cudaSuccess;
+    if (e == cudaSuccess) e = cudaEventRecord(b->fork, b->cs);
+    for (int i = 0; e == cudaSuccess && i < ns; ++i) e = cudaStreamWaitEvent(b->side[i], b->fork, 0);
+    for (int i = 0; e == cudaSuccess && !rc && i < nm; ++i) rc = batch_enqueue(b, order[i], b->side[i % ns], screened);
+    for (int i = 0; e == cudaSuccess && !rc && i < ns; ++i) {
+        e = cudaEventRecord(b->join[i], b->side[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cs, b->join[i], 0);
+    }
+    *g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(b->cs, g);
+    if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+        if (*g) cudaGraphDestroy(*g);
+        *g = nullptr;
+        if (rc) return rc;
+        return fail(PATGPU_ECUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    if (cudaGraphInstantiate(x, *g, 0) != cudaSuccess) {
+        cudaGraphDestroy(*g);
+        *g = nullptr;
+        return fail(PATGPU_ECUDA, "batch graph instantiation failed");
+    }
+    return 0;
+}
+
+// Capture graph [k] (0: plain builds, 1: density-screened builds).  The
+// first capture of each kind also chooses how many side streams the
+// molecules are spread over: all of them (molecules run side by side and
+// fill each other's tails) or one (each launch has the GPU to itself; the
+// class kernels' grids already fill every SM once).  Both graphs are timed
+// on one launch each over the buffers' current densities and the faster is
+// kept, and the choice holds for later captures of that kind.
 static int batch_capture(patgpu_batch_s *b, int k)
 {
     const bool screened = k == 1;
@@ -2141,34 +2190,36 @@ static int batch_capture(patgpu_batch_s *b, int k)
         if (rc) return rc;
     }
     PG_CUDA(cudaStreamSynchronize(b->cs));
-    // heaviest molecules first, dealt round-robin over the capture streams
-    std::vector<int> order(nm);
-    for (int m = 0; m < nm; ++m) order[m] = m;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int x, int y) { return b->mols[x]->nquart > b->mols[y]->nquart; });
-    PG_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
-    int rc = 0;
-    // graph [1] first copies the current thresholds from the pinned pair
-    cudaError_t e = screened ? cudaMemcpyAsync(b->d_scr.p, b->h_scr, scr_bytes, cudaMemcpyHostToDevice, b->cs)
-                             : cudaSuccess;
-    if (e == cudaSuccess) e = cudaEventRecord(b->fork, b->cs);
-    for (size_t i = 0; e == cudaSuccess && i < b->side.size(); ++i) e = cudaStreamWaitEvent(b->side[i], b->fork, 0);
-    for (int i = 0; e == cudaSuccess && !rc && i < nm; ++i) rc = batch_enqueue(b, order[i], b->side[i % b->side.size()], screened);
-    for (size_t i = 0; e == cudaSuccess && !rc && i < b->side.size(); ++i) {
-        e = cudaEventRecord(b->join[i], b->side[i]);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cs, b->join[i], 0);
-    }
-    cudaGraph_t g = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(b->cs, &g);
-    if (rc || e != cudaSuccess || e2 != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
+    const int all = (int)b->side.size();
+    if (b->nside[k] > 0 || all == 1) {
+        const int ns = b->nside[k] > 0 ? b->nside[k] : all;
+        if (int rc = batch_capture_streams(b, k, ns, &b->graph[k], &b->exec[k])) return rc;
+    } else {
+        cudaGraph_t g[2] = {nullptr, nullptr};
+        cudaGraphExec_t x[2] = {nullptr, nullptr};
+        const int ns[2] = {all, 1};
+        float ms[2] = {0.f, 0.f};
+        int rc = 0;
+        for (int c = 0; c < 2 && !rc; ++c) {
+            rc = batch_capture_streams(b, k, ns[c], &g[c], &x[c]);
+            if (!rc && (cudaEventRecord(b->ev0, b->cs) != cudaSuccess || cudaGraphLaunch(x[c], b->cs) != cudaSuccess ||
+                        cudaEventRecord(b->ev1, b->cs) != cudaSuccess || cudaEventSynchronize(b->ev1) != cudaSuccess ||
+                        cudaEventElapsedTime(&ms[c], b->ev0, b->ev1) != cudaSuccess))
+                rc = fail(PATGPU_ECUDA, "batch stream-count trial failed");
+        }
+        const int keep = (!rc && ms[1] < ms[0]) ? 1 : 0;
+        for (int c = 0; c < 2; ++c) {
+            if (c == keep && !rc) continue;
+            if (x[c]) cudaGraphExecDestroy(x[c]);
+            if (g[c]) cudaGraphDestroy(g[c]);
+        }
         if (rc) return rc;
-        return fail(PATGPU_ECUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        b->graph[k] = g[keep];
+        b->exec[k] = x[keep];
+        b->nside[k] = ns[keep];
     }
-    b->graph[k] = g;
-    PG_CUDA(cudaGraphInstantiate(&b->exec[k], g, 0));
     size_t nodes = 0;
-    PG_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+    PG_CUDA(cudaGraphGetNodes(b->graph[k], nullptr, &nodes));
     b->nodes[k] = (int)nodes;
     return 0;
 }
@@ -2343,13 +2394,14 @@ int patgpu_batch_rhf_gmatrix(patgpu_batch b, const double *const *P, double *con
         if (!P[m] || !G[m]) return fail(PATGPU_EINVAL, "patgpu_batch_rhf_gmatrix: molecule %d has no matrix", m);
         tot += (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
     }
-    if (!b->exec[b->screened]) {
-        int rc = batch_capture(b, b->screened);
-        if (rc) return rc;
-    }
+    // densities first: a first capture times its graphs over them
     for (int m = 0; m < nm; ++m) {
         const size_t no2 = (size_t)b->mols[m]->n * (b->mols[m]->n + 1) / 2;
         PG_CUDA(cudaMemcpyAsync(b->dP[m].p, P[m], sizeof(double) * no2, cudaMemcpyHostToDevice, b->cs));
+    }
+    if (!b->exec[b->screened]) {
+        int rc = batch_capture(b, b->screened);
+        if (rc) return rc;
     }
     int rc = patgpu_batch_launch(b, b->cs);
     if (rc) return rc;
