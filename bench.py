@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--scf-tau-rel", type=float, default=1e-6,
                     help="SCF-iteration leg: screening of the mixed batch's builds at this times the largest DIIS "
                          "error, clipped to [--scf-tau-inc, --scf-tau-max] (0: fixed --scf-tau-inc)")
-    ap.add_argument("--scf-tau-max", type=float, default=1e-8)
+    ap.add_argument("--scf-tau-max", type=float, default=1e-7)
     ap.add_argument("--scf-ediis", type=int, default=1,
                     help="SCF-iteration leg: 1 blends energy-DIIS into DIIS while the DIIS error is above 1e-4")
     ap.add_argument("--scf-molecules", type=int, default=8,

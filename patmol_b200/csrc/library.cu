@@ -872,7 +872,7 @@ static int tune_fp32(patgpu_basis *h)
             if (h->single_prim && eri_has_variant(w.la, w.lb, w.lc, w.ld, 7)) w.variant32 = 7;
         return 0;
     }
-    // timed on the Schwarz FP32 window, or, when only the density-weighted
+    // timed on the FP32 (term-bound) window, or, when only the density-weighted
     // window of difference builds is set, on the class's whole list
     const bool schwarz_window = h->tau_mix > 0.0;
     if (h->work.empty() || !h->lists || (!schwarz_window && h->tau_dens32 <= 0.0)) return 0;
