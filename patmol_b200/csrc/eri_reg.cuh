@@ -87,55 +87,89 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
          qi += (long long)gridDim.x * blockDim.x) {
         int u, v;
         if (!eri_quartet_at(args, q0 + qi, u, v)) continue;
-        const int npb = args.pr.pnum[u], npk = args.pr.pnum[v];
-        const int pb0 = args.pr.pstart[u], pk0 = args.pr.pstart[v];
-        const double ax = args.pr.ax[u], ay = args.pr.ay[u], az = args.pr.az[u];
-        const double abx = args.pr.abx[u], aby = args.pr.aby[u], abz = args.pr.abz[u];
-        const double cx = args.pr.ax[v], cy = args.pr.ay[v], cz = args.pr.az[v];
-        const double cdx = args.pr.abx[v], cdy = args.pr.aby[v], cdz = args.pr.abz[v];
+        double ax, ay, az, abx, aby, abz, cx, cy, cz, cdx, cdy, cdz;
+        int fa, fb, fc, fd;
+        bool sab, scd;
 
         double I[NCART];
 #pragma unroll
         for (int c = 0; c < NCART; ++c) I[c] = 0.0;
 
-        for (int ib = pb0; ib < pb0 + npb; ++ib)
-            for (int ik = pk0; ik < pk0 + npk; ++ik) {
-                const double p = args.pp.p[ib], qx = args.pp.p[ik];
-                const double ppq = p + qx, rs = rsqrt(ppq);
-                if (kSR * args.pp.cut[ib] * args.pp.cut[ik] * rs < args.prim_cut) continue;   // twoints.c:109-111
-                const double sr = kSR * args.pp.K[ib] * args.pp.K[ik] * rs;
-                const double Px = args.pp.px[ib], Py = args.pp.py[ib], Pz = args.pp.pz[ib];
-                const double Qx = args.pp.px[ik], Qy = args.pp.py[ik], Qz = args.pp.pz[ik];
-                const double pax = Px - ax, pay = Py - ay, paz = Pz - az;
-                const double qcx = Qx - cx, qcy = Qy - cy, qcz = Qz - cz;
-                const double pqx = Px - Qx, pqy = Py - Qy, pqz = Pz - Qz;
-                const double T = p * qx / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
+        // one primitive quartet: p, P, K, the coefficient-free prefactor of
+        // the bra pair, the same of the ket pair
+        auto prim = [&](double p, double Px, double Py, double Pz, double Kb, double cb, double qx, double Qx,
+                        double Qy, double Qz, double Kk, double ck) {
+            const double ppq = p + qx, rs = rsqrt(ppq);
+            if (kSR * cb * ck * rs < args.prim_cut) return;   // twoints.c:109-111
+            const double sr = kSR * Kb * Kk * rs;
+            const double pax = Px - ax, pay = Py - ay, paz = Pz - az;
+            const double qcx = Qx - cx, qcy = Qy - cy, qcz = Qz - cz;
+            const double pqx = Px - Qx, pqy = Py - Qy, pqz = Pz - Qz;
+            const double T = p * qx / ppq * (pqx * pqx + pqy * pqy + pqz * pqz);
 #pragma unroll 1
-                for (int r = 0; r < NR; ++r) {
-                    const double x = rys_eval(NR, r, T, c_rys, args.rys_coef, kRysDeg, true);
-                    const double w = rys_eval(NR, NR + r, T, c_rys, args.rys_coef, kRysDeg, true);
-                    const double f = x / ppq, B00 = 0.5 * f;
-                    const double B10 = (0.5 - B00 * qx) / p, B01 = (0.5 - B00 * p) / qx;
-                    double tx[TSZ], ty[TSZ], tz[TSZ];
-                    vrr_hrr_reg<LA, LB, LC, LD>(tx, 1.0, B00, B10, B01, pax - qx * pqx * f, qcx + p * pqx * f, abx, cdx);
-                    vrr_hrr_reg<LA, LB, LC, LD>(ty, 1.0, B00, B10, B01, pay - qx * pqy * f, qcy + p * pqy * f, aby, cdy);
-                    vrr_hrr_reg<LA, LB, LC, LD>(tz, w * sr, B00, B10, B01, paz - qx * pqz * f, qcz + p * pqz * f, abz,
-                                                cdz);
+            for (int r = 0; r < NR; ++r) {
+                const double x = rys_eval(NR, r, T, c_rys, args.rys_coef, kRysDeg, true);
+                const double w = rys_eval(NR, NR + r, T, c_rys, args.rys_coef, kRysDeg, true);
+                const double f = x / ppq, B00 = 0.5 * f;
+                const double B10 = (0.5 - B00 * qx) / p, B01 = (0.5 - B00 * p) / qx;
+                double tx[TSZ], ty[TSZ], tz[TSZ];
+                vrr_hrr_reg<LA, LB, LC, LD>(tx, 1.0, B00, B10, B01, pax - qx * pqx * f, qcx + p * pqx * f, abx, cdx);
+                vrr_hrr_reg<LA, LB, LC, LD>(ty, 1.0, B00, B10, B01, pay - qx * pqy * f, qcy + p * pqy * f, aby, cdy);
+                vrr_hrr_reg<LA, LB, LC, LD>(tz, w * sr, B00, B10, B01, paz - qx * pqz * f, qcz + p * pqz * f, abz,
+                                            cdz);
 #pragma unroll
-                    for (int ab = 0; ab < NAB; ++ab)
+                for (int ab = 0; ab < NAB; ++ab)
 #pragma unroll
-                        for (int cd = 0; cd < NCD; ++cd) {
-                            const int ia = ab / NB, ib2 = ab % NB, ic = cd / ND, id = cd % ND;
-                            const int ox = (cexp(LC, ic, 0) * (LD + 1) + cexp(LD, id, 0)) * TAB +
-                                           cexp(LA, ia, 0) * (LB + 1) + cexp(LB, ib2, 0);
-                            const int oy = (cexp(LC, ic, 1) * (LD + 1) + cexp(LD, id, 1)) * TAB +
-                                           cexp(LA, ia, 1) * (LB + 1) + cexp(LB, ib2, 1);
-                            const int oz = (cexp(LC, ic, 2) * (LD + 1) + cexp(LD, id, 2)) * TAB +
-                                           cexp(LA, ia, 2) * (LB + 1) + cexp(LB, ib2, 2);
-                            I[ab * NCD + cd] = fma(tx[ox] * ty[oy], tz[oz], I[ab * NCD + cd]);
-                        }
-                }
+                    for (int cd = 0; cd < NCD; ++cd) {
+                        const int ia = ab / NB, ib2 = ab % NB, ic = cd / ND, id = cd % ND;
+                        const int ox = (cexp(LC, ic, 0) * (LD + 1) + cexp(LD, id, 0)) * TAB +
+                                       cexp(LA, ia, 0) * (LB + 1) + cexp(LB, ib2, 0);
+                        const int oy = (cexp(LC, ic, 1) * (LD + 1) + cexp(LD, id, 1)) * TAB +
+                                       cexp(LA, ia, 1) * (LB + 1) + cexp(LB, ib2, 1);
+                        const int oz = (cexp(LC, ic, 2) * (LD + 1) + cexp(LD, id, 2)) * TAB +
+                                       cexp(LA, ia, 2) * (LB + 1) + cexp(LB, ib2, 2);
+                        I[ab * NCD + cd] = fma(tx[ox] * ty[oy], tz[oz], I[ab * NCD + cd]);
+                    }
             }
+        };
+
+        if (args.ppk) {
+            // one-primitive handles: each pair is one 128-byte record
+            // (EriArgs::ppk) read with seven 128-bit loads, instead of
+            // fourteen scattered words of the pair and primitive arrays
+            const double2 *Rb = reinterpret_cast<const double2 *>(args.ppk) + 8 * (size_t)u;
+            const double2 *Rk = reinterpret_cast<const double2 *>(args.ppk) + 8 * (size_t)v;
+            const double2 b0 = __ldg(Rb), b1 = __ldg(Rb + 1), b2 = __ldg(Rb + 2), b3 = __ldg(Rb + 3);
+            const double2 b4 = __ldg(Rb + 4), b5 = __ldg(Rb + 5), b6 = __ldg(Rb + 6);
+            const double2 k0 = __ldg(Rk), k1 = __ldg(Rk + 1), k2 = __ldg(Rk + 2), k3 = __ldg(Rk + 3);
+            const double2 k4 = __ldg(Rk + 4), k5 = __ldg(Rk + 5), k6 = __ldg(Rk + 6);
+            ax = b3.x; ay = b3.y; az = b4.x; abx = b4.y; aby = b5.x; abz = b5.y;
+            cx = k3.x; cy = k3.y; cz = k4.x; cdx = k4.y; cdy = k5.x; cdz = k5.y;
+            const unsigned long long fab = (unsigned long long)__double_as_longlong(b6.x);
+            const unsigned long long fcd = (unsigned long long)__double_as_longlong(k6.x);
+            const unsigned long long sb2 = (unsigned long long)__double_as_longlong(b6.y);
+            const unsigned long long sk2 = (unsigned long long)__double_as_longlong(k6.y);
+            fa = (int)(unsigned)(fab & 0xffffffffull); fb = (int)(unsigned)(fab >> 32);
+            fc = (int)(unsigned)(fcd & 0xffffffffull); fd = (int)(unsigned)(fcd >> 32);
+            sab = (sb2 & 0xffffffffull) == (sb2 >> 32);
+            scd = (sk2 & 0xffffffffull) == (sk2 >> 32);
+            prim(b0.x, b0.y, b1.x, b1.y, b2.x, b2.y, k0.x, k0.y, k1.x, k1.y, k2.x, k2.y);
+        } else {
+            ax = args.pr.ax[u]; ay = args.pr.ay[u]; az = args.pr.az[u];
+            abx = args.pr.abx[u]; aby = args.pr.aby[u]; abz = args.pr.abz[u];
+            cx = args.pr.ax[v]; cy = args.pr.ay[v]; cz = args.pr.az[v];
+            cdx = args.pr.abx[v]; cdy = args.pr.aby[v]; cdz = args.pr.abz[v];
+            fa = args.pr.fa[u]; fb = args.pr.fb[u]; fc = args.pr.fa[v]; fd = args.pr.fb[v];
+            sab = args.pr.sa[u] == args.pr.sb[u];
+            scd = args.pr.sa[v] == args.pr.sb[v];
+            const int npb = args.pr.pnum[u], npk = args.pr.pnum[v];
+            const int pb0 = args.pr.pstart[u], pk0 = args.pr.pstart[v];
+            for (int ib = pb0; ib < pb0 + npb; ++ib)
+                for (int ik = pk0; ik < pk0 + npk; ++ik)
+                    prim(args.pp.p[ib], args.pp.px[ib], args.pp.py[ib], args.pp.pz[ib], args.pp.K[ib],
+                         args.pp.cut[ib], args.pp.p[ik], args.pp.px[ik], args.pp.py[ik], args.pp.pz[ik],
+                         args.pp.K[ik], args.pp.cut[ik]);
+        }
 
         if (mode == MODE_EXPORT) {
             double *o = args.out + args.out_off[qi];
@@ -158,8 +192,6 @@ __global__ void __launch_bounds__(128, 4) eri_reg_kernel(const EriArgs args)
                 I[ab * NCD + cd] *= c_norm[LA][ab / NB] * c_norm[LB][ab % NB] * c_norm[LC][cd / ND] *
                                     c_norm[LD][cd % ND];
 
-        const int fa = args.pr.fa[u], fb = args.pr.fb[u], fc = args.pr.fa[v], fd = args.pr.fb[v];
-        const bool sab = args.pr.sa[u] == args.pr.sb[u], scd = args.pr.sa[v] == args.pr.sb[v];
         const double deg = (sab ? 1.0 : 2.0) * (scd ? 1.0 : 2.0) * (u == v ? 1.0 : 2.0);
         const double sJ = mode == MODE_RHF ? 0.5 * deg : 0.25 * deg;
         const double sK = 0.125 * deg;
