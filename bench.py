@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--batch-max-atoms", type=int, default=8,
                     help="molecule sizes of the batched leg are uniform in 3..this")
     ap.add_argument("--alkane-carbons", type=int, default=12)
-    ap.add_argument("--scf-maxit", type=int, default=40, help="SCF-iteration leg: iteration cap of both forms")
+    ap.add_argument("--scf-maxit", type=int, default=50, help="SCF-iteration leg: iteration cap of both forms")
     ap.add_argument("--scf-tau-inc", type=float, default=1e-11,
                     help="SCF-iteration leg: density screening of the mixed batch's difference builds")
     ap.add_argument("--scf-tau-rel", type=float, default=1e-6,
