@@ -110,7 +110,9 @@ class _RHFState:
         G = unpack(Gp, self.n)
         F = self.H + G
         energy = 2.0 * np.sum(self.P * self.H) + np.sum(self.P * G) + self.enuc
-        err = F @ self.P @ self.S - self.S @ self.P @ F
+        # F, P and S are symmetric, so S P F = (F P S)^T: two GEMMs, not four
+        FPS = F @ self.P @ self.S
+        err = FPS - FPS.T
         self.fs.append(F)
         self.es.append(self.X.T @ err @ self.X)
         if self.ediis:
@@ -428,7 +430,8 @@ def uhf(basis: Basis, dpm: bool = False, gpu: GpuBasis | None = None, conv: floa
         G = [unpack(GA, n), unpack(GB, n)]
         F = [H + G[0], H + G[1]]
         energy = sum(np.sum(P[s] * H) + 0.5 * np.sum(P[s] * G[s]) for s in range(2)) + enuc
-        errs = [X.T @ (F[s] @ P[s] @ S - S @ P[s] @ F[s]) @ X for s in range(2)]
+        FPS = [F[s] @ P[s] @ S for s in range(2)]
+        errs = [X.T @ (FPS[s] - FPS[s].T) @ X for s in range(2)]   # S P F = (F P S)^T
         hist_f.append(F)
         hist_e.append(errs)
         hist_f, hist_e = hist_f[-ndiis:], hist_e[-ndiis:]
