@@ -85,6 +85,7 @@ class _RHFState:
         self.linalg = GpuScfLinalg(self.X, self.nocc) if device_linalg else None
         self.eps, C, self.P = self.diag_density(self.H)
         self.fs, self.es = [], []
+        self.eov = np.zeros((0, 0))
         self.e_old = None
         self.converged = False
         self.it = 0
@@ -114,18 +115,25 @@ class _RHFState:
         FPS = F @ self.P @ self.S
         err = FPS - FPS.T
         self.fs.append(F)
-        self.es.append(self.X.T @ err @ self.X)
+        e_new = self.X.T @ err @ self.X
+        self.es.append(e_new)
+        # the error overlaps <e_i, e_j>: one new row a step, the oldest
+        # dropped with its vectors
+        m0 = self.eov.shape[0]
+        eov = np.zeros((m0 + 1, m0 + 1))
+        eov[:m0, :m0] = self.eov
+        for j in range(m0 + 1):
+            eov[m0, j] = eov[j, m0] = np.sum(e_new * self.es[len(self.es) - 1 - m0 + j])
         if self.ediis:
             self._ediis_push(self.P, F, energy)
         self.fs, self.es = self.fs[-self.ndiis:], self.es[-self.ndiis:]
+        self.eov = eov[-len(self.es):, -len(self.es):]
         F_last = F
         if len(self.fs) > 1:
             m = len(self.fs)
             B = -np.ones((m + 1, m + 1))
             B[m, m] = 0.0
-            for i in range(m):
-                for j in range(m):
-                    B[i, j] = np.sum(self.es[i] * self.es[j])
+            B[:m, :m] = self.eov
             rhs = np.zeros(m + 1)
             rhs[m] = -1.0
             try:
